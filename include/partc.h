@@ -1,0 +1,160 @@
+/*
+ * partc.h -- C ABI of the B200 sparse tensor contraction engine (parTC's fksCuckooTC path).
+ *
+ * parTC's driver (main.cpp:115-118) builds two FKS/cuckoo hash tables and calls
+ *     Tensor tc_fksCuckoo(Hash_Table* HT_A, Hash_Table* HT_B, Tensor& A_copy, Tensor& B);
+ * (fksCuckooTC.hpp:80).  This header replaces those three calls with one entry point that takes
+ * the same COO arrays (tensor.hpp:19-27: hedges_array = 0-based u32 indices, AoS, N x d;
+ * val_array = f64; dimensions_array; dim_tc = contracted modes first) and returns the same
+ * output tensor (u32 AoS indices, A's free modes then B's free modes, and f64 values).
+ *
+ * Differences in error behaviour: where the reference calls exit(), these functions return a
+ * status code (see ptc_status); ptc_last_error() gives the message.  Functions are thread-safe;
+ * the last error is kept per host thread.
+ */
+#ifndef PARTC_H
+#define PARTC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PTC_API_VERSION 1
+
+typedef enum ptc_status {
+    PTC_OK = 0,
+    PTC_ERR_INVALID_ARGUMENT = 1, /* null pointer, bad order / mode list / sizes */
+    PTC_ERR_INDEX_RANGE = 2,      /* an index is >= its mode size */
+    PTC_ERR_KEY_OVERFLOW = 3,     /* product of the contracted (or free) mode sizes >= 2^64 */
+    PTC_ERR_EMPTY_CONTRACTION = 4,/* no A nonzero meets a B fiber; the reference exits with
+                                     "tensor contraction not possible!!" (tensor.hpp:116-119) */
+    PTC_ERR_TOO_FEW_NONZEROS = 5, /* self-contraction of a tensor with <= 1 nonzero; the reference
+                                     exits with "Tensor B has at most one nonzeros!!"
+                                     (sparse_tensor_generator.hpp:18-21) */
+    PTC_ERR_HASH_BUILD = 6,       /* cuckoo build failed after every reseed/growth; the reference
+                                     exits with "None of the keys in kDict worked"
+                                     (fksCuckoo.hpp:439-441) */
+    PTC_ERR_OUT_OF_MEMORY = 7,    /* device or host allocation failed (reference: exit(1),
+                                     fksCuckoo.hpp:244-247) */
+    PTC_ERR_CUDA = 8,             /* a CUDA runtime call failed */
+    PTC_ERR_NO_DEVICE = 9,        /* no usable sm_100 device */
+    PTC_ERR_DEVICE_TIMEOUT = 10,  /* a bounded device-side wait gave up */
+    PTC_ERR_OVERFLOW = 11,        /* a result does not fit the caller-provided capacity */
+    PTC_ERR_INTERNAL = 12
+} ptc_status;
+
+/* where a buffer lives */
+enum { PTC_HOST = 0, PTC_DEVICE = 1 };
+
+/* which numeric path to run */
+enum {
+    PTC_PATH_TWO_PHASE = 0, /* exact symbolic pass (per-row output nnz), then numeric pass */
+    PTC_PATH_LEARNED = 1    /* learned sizer replaces the symbolic pass; rows that overflow
+                               their predicted accumulator rerun exactly */
+};
+
+/* COO input tensor (the reference's Tensor, tensor.hpp:19-27). */
+typedef struct ptc_coo {
+    uint32_t order;        /* d */
+    uint32_t location;     /* PTC_HOST or PTC_DEVICE, for idx and vals */
+    uint64_t nnz;          /* N */
+    const uint32_t* idx;   /* [nnz * order], 0-based, AoS (hedges_array) */
+    const double* vals;    /* [nnz] (val_array) */
+    const uint32_t* dims;  /* [order] mode sizes, host memory (dimensions_array) */
+} ptc_coo;
+
+/* Output tensor (the Tensor returned by tc_fksCuckoo, fksCuckooTC.hpp:156,360). */
+typedef struct ptc_tensor {
+    uint32_t order;        /* (A free modes) + (B free modes) */
+    uint32_t location;     /* PTC_HOST or PTC_DEVICE */
+    uint64_t nnz;          /* O.N */
+    uint32_t* idx;         /* [nnz * order] */
+    double* vals;          /* [nnz] */
+    void* opaque;          /* owned by the library; release with ptc_tensor_free */
+} ptc_tensor;
+
+typedef struct ptc_sizer ptc_sizer; /* learned output-size predictor (opaque) */
+
+typedef struct ptc_options {
+    uint32_t struct_size;      /* sizeof(ptc_options) */
+    int32_t device;            /* CUDA device ordinal; -1 = current device */
+    void* stream;              /* cudaStream_t to run on; NULL = the library's own stream */
+    uint32_t path;             /* PTC_PATH_TWO_PHASE (default) or PTC_PATH_LEARNED */
+    uint32_t output_location;  /* PTC_HOST (default, like the reference) or PTC_DEVICE */
+    uint32_t verbose;          /* 1: print the reference's stdout lines (timings, nnz) */
+    uint32_t panel_width;      /* columns per dense accumulator panel; 0 = automatic */
+    uint64_t hash_seed;        /* seed of the cuckoo hash family */
+    const ptc_sizer* sizer;    /* PTC_PATH_LEARNED: trained sizer (NULL = built-in weights) */
+    uint32_t sort_rows;        /* 1: rows of the output in increasing free-key order and every
+                                  row in increasing column order (canonical COO) */
+    uint32_t reserved[7];
+} ptc_options;
+
+/* Per-call statistics; every time is measured with CUDA events on the call's stream. */
+typedef struct ptc_stats {
+    uint64_t mult_adds;        /* sum over A nonzeros of the matching B fiber's length */
+    uint64_t out_nnz;
+    uint64_t nrows;            /* distinct A free keys (rows of HT_A) */
+    uint64_t ncols;            /* distinct B free keys */
+    uint64_t nfibers;          /* distinct B contracted keys (fibers of HT_B) */
+    uint64_t a_nnz, b_nnz;
+    double t_total_ms;         /* whole call */
+    double t_h2d_ms;           /* host-to-device input copies */
+    double t_build_ms;         /* keys, sorts, cuckoo build, probes (HT_B + HT_A + reorder) */
+    double t_symbolic_ms;      /* exact symbolic pass, or sizer features + inference */
+    double t_numeric_ms;       /* numeric pass incl. output writes (the reference's
+                                  "Total time for tensor contraction") */
+    double t_d2h_ms;           /* device-to-host output copies */
+    uint32_t hash_attempts;    /* cuckoo builds tried (1 = first seed worked) */
+    uint32_t panel_width;      /* dense panel width used */
+    uint64_t rows_small, rows_hash, rows_panel, rows_long; /* rows per accumulator bin */
+    uint64_t rerun_rows;       /* learned path: rows rerun exactly after an overflow */
+    double sizer_mean_abs_log2_err; /* learned path: mean |log2(pred/actual)| over rows */
+    uint64_t kernel_launches;  /* kernels this call launched */
+    double reserved[4];
+} ptc_stats;
+
+/* Fill *opt with defaults. */
+void ptc_options_init(ptc_options* opt);
+
+/* Human-readable message of the last failing call on this host thread. */
+const char* ptc_last_error(void);
+
+/* Status code name. */
+const char* ptc_status_string(ptc_status s);
+
+/*
+ * O = A x B over c contracted modes.  a_modes[0..c) and b_modes[0..c) are the contracted modes
+ * (paired in order); a_modes[c..order_A) and b_modes[c..order_B) are the free modes in output
+ * order -- the dim_tc arrays of the reference (meta file line 2).  B == NULL means B = A with
+ * b_modes = a_modes: the reference's self-contraction (main.cpp:112,
+ * sparse_tensor_generator.hpp:4-88).  Replaces main.cpp:115-118.
+ * The output is allocated by the library (host malloc or device memory per
+ * opt->output_location) and must be released with ptc_tensor_free.
+ */
+ptc_status ptc_contract(const ptc_coo* A, const ptc_coo* B, uint32_t c, const uint32_t* a_modes,
+                        const uint32_t* b_modes, const ptc_options* opt, ptc_tensor* out,
+                        ptc_stats* stats);
+
+/*
+ * The self-contraction exactly as main.cpp calls it: the tensor's arrays as read by readTensor
+ * (mtxTnsIO.cpp:30-65), c and dim_tc as read by Tensor::populate_meta_info (tensor.hpp:151-173).
+ * Equivalent to ptc_contract(&A, NULL, c, dim_tc, dim_tc, ...).  Replaces main.cpp:112-118.
+ */
+ptc_status ptc_self_contract(const uint32_t* hedges, const double* vals, uint32_t d, uint64_t N,
+                             const uint32_t* dims, uint32_t c, const uint32_t* dim_tc,
+                             const ptc_options* opt, ptc_tensor* out, ptc_stats* stats);
+
+/* Release an output tensor made by this library. */
+void ptc_tensor_free(ptc_tensor* t);
+
+/* Number of CUDA devices the library can use (sm_100 class). */
+int ptc_device_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PARTC_H */

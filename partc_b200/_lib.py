@@ -1,0 +1,185 @@
+"""ctypes binding of the engine's C ABI (``include/partc.h``).
+
+The CUDA library ``libpartc_b200.so`` is the product; this module only loads it and converts
+numpy arrays.  There is no CPU fallback: if the library is missing or no B200 is visible, calls
+fail loudly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libpartc_b200.so")
+
+PTC_HOST, PTC_DEVICE = 0, 1
+PATH_TWO_PHASE, PATH_LEARNED = 0, 1
+
+STATUS = {
+    0: "PTC_OK", 1: "PTC_ERR_INVALID_ARGUMENT", 2: "PTC_ERR_INDEX_RANGE", 3: "PTC_ERR_KEY_OVERFLOW",
+    4: "PTC_ERR_EMPTY_CONTRACTION", 5: "PTC_ERR_TOO_FEW_NONZEROS", 6: "PTC_ERR_HASH_BUILD",
+    7: "PTC_ERR_OUT_OF_MEMORY", 8: "PTC_ERR_CUDA", 9: "PTC_ERR_NO_DEVICE", 10: "PTC_ERR_DEVICE_TIMEOUT",
+    11: "PTC_ERR_OVERFLOW", 12: "PTC_ERR_INTERNAL",
+}
+
+# every function include/partc.h declares (checked by the CPU tests)
+EXPORTS = [
+    "ptc_options_init", "ptc_last_error", "ptc_status_string", "ptc_contract", "ptc_self_contract",
+    "ptc_tensor_free", "ptc_device_count",
+]
+
+
+class PtcError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+        self.name = STATUS.get(status, str(status))
+
+
+class Coo(C.Structure):
+    _fields_ = [("order", C.c_uint32), ("location", C.c_uint32), ("nnz", C.c_uint64),
+                ("idx", C.c_void_p), ("vals", C.c_void_p), ("dims", C.c_void_p)]
+
+
+class Tensor(C.Structure):
+    _fields_ = [("order", C.c_uint32), ("location", C.c_uint32), ("nnz", C.c_uint64),
+                ("idx", C.POINTER(C.c_uint32)), ("vals", C.POINTER(C.c_double)), ("opaque", C.c_void_p)]
+
+
+class Options(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("device", C.c_int32), ("stream", C.c_void_p),
+                ("path", C.c_uint32), ("output_location", C.c_uint32), ("verbose", C.c_uint32),
+                ("panel_width", C.c_uint32), ("hash_seed", C.c_uint64), ("sizer", C.c_void_p),
+                ("sort_rows", C.c_uint32), ("reserved", C.c_uint32 * 7)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("mult_adds", C.c_uint64), ("out_nnz", C.c_uint64), ("nrows", C.c_uint64),
+                ("ncols", C.c_uint64), ("nfibers", C.c_uint64), ("a_nnz", C.c_uint64), ("b_nnz", C.c_uint64),
+                ("t_total_ms", C.c_double), ("t_h2d_ms", C.c_double), ("t_build_ms", C.c_double),
+                ("t_symbolic_ms", C.c_double), ("t_numeric_ms", C.c_double), ("t_d2h_ms", C.c_double),
+                ("hash_attempts", C.c_uint32), ("panel_width", C.c_uint32),
+                ("rows_small", C.c_uint64), ("rows_hash", C.c_uint64), ("rows_panel", C.c_uint64),
+                ("rows_long", C.c_uint64), ("rerun_rows", C.c_uint64), ("sizer_mean_abs_log2_err", C.c_double),
+                ("kernel_launches", C.c_uint64), ("reserved", C.c_double * 4)]
+
+    def as_dict(self) -> dict:
+        return {name: (getattr(self, name) if not name == "reserved" else None)
+                for name, _ in self._fields_ if name != "reserved"}
+
+
+_lib = None
+
+
+def lib():
+    """Load the CUDA library (built by ``python -m partc_b200.build``)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing; build it with `python -m partc_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        L.ptc_options_init.argtypes = [C.POINTER(Options)]
+        L.ptc_options_init.restype = None
+        L.ptc_last_error.restype = C.c_char_p
+        L.ptc_status_string.argtypes = [C.c_int]
+        L.ptc_status_string.restype = C.c_char_p
+        L.ptc_contract.argtypes = [C.POINTER(Coo), C.POINTER(Coo), C.c_uint32, C.c_void_p, C.c_void_p,
+                                   C.POINTER(Options), C.POINTER(Tensor), C.POINTER(Stats)]
+        L.ptc_contract.restype = C.c_int
+        L.ptc_self_contract.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64, C.c_void_p, C.c_uint32,
+                                        C.c_void_p, C.POINTER(Options), C.POINTER(Tensor), C.POINTER(Stats)]
+        L.ptc_self_contract.restype = C.c_int
+        L.ptc_tensor_free.argtypes = [C.POINTER(Tensor)]
+        L.ptc_tensor_free.restype = None
+        L.ptc_device_count.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def options(**kw) -> Options:
+    o = Options()
+    lib().ptc_options_init(C.byref(o))
+    for k, v in kw.items():
+        if k == "path" and isinstance(v, str):
+            v = {"two_phase": PATH_TWO_PHASE, "learned": PATH_LEARNED}[v]
+        if k == "output_location" and isinstance(v, str):
+            v = {"host": PTC_HOST, "device": PTC_DEVICE}[v]
+        setattr(o, k, v)
+    return o
+
+
+def _check(rc: int):
+    if rc != 0:
+        raise PtcError(rc, lib().ptc_last_error().decode())
+
+
+def _host_coo(t, keep: list) -> Coo:
+    idx = np.ascontiguousarray(t.idx, dtype=np.uint32)
+    vals = np.ascontiguousarray(t.vals, dtype=np.float64)
+    dims = np.ascontiguousarray(t.dims, dtype=np.uint32)
+    keep += [idx, vals, dims]
+    order = idx.shape[1] if idx.ndim == 2 else len(dims)
+    return Coo(order, PTC_HOST, idx.shape[0] if idx.ndim == 2 else 0, idx.ctypes.data, vals.ctypes.data,
+               dims.ctypes.data)
+
+
+def device_coo(idx_ptr: int, vals_ptr: int, nnz: int, dims, keep: list) -> Coo:
+    """Describe a tensor whose idx/vals already live in device memory (e.g. torch CUDA tensors)."""
+    d = np.ascontiguousarray(dims, dtype=np.uint32)
+    keep.append(d)
+    return Coo(len(d), PTC_DEVICE, nnz, idx_ptr, vals_ptr, d.ctypes.data)
+
+
+def contract(A, B=None, c: int = 1, a_modes=None, b_modes=None, *, keep_device: bool = False, **opt):
+    """O = A x B through ``ptc_contract`` with host inputs.  Returns ``(idx, vals, stats)``:
+    ``idx`` is ``uint32[nnz, order]``.  With ``keep_device=True`` the output stays on the device
+    and a raw ``Tensor`` struct is returned instead of arrays (free it with :func:`free`)."""
+    L = lib()
+    keep: list = []
+    ca = _host_coo(A, keep)
+    cb = None if B is None else _host_coo(B, keep)
+    am = np.ascontiguousarray(a_modes, dtype=np.uint32)
+    bm = am if b_modes is None else np.ascontiguousarray(b_modes, dtype=np.uint32)
+    if keep_device:
+        opt.setdefault("output_location", PTC_DEVICE)
+    o = options(**opt)
+    out = Tensor()
+    st = Stats()
+    rc = L.ptc_contract(C.byref(ca), None if cb is None else C.byref(cb), c, am.ctypes.data, bm.ctypes.data,
+                        C.byref(o), C.byref(out), C.byref(st))
+    _check(rc)
+    if o.output_location == PTC_DEVICE:
+        return out, None, st.as_dict()
+    try:
+        n, d = out.nnz, out.order
+        idx = np.ctypeslib.as_array(out.idx, shape=(n * d,)).reshape(n, d).copy() if n else np.zeros((0, d), np.uint32)
+        vals = np.ctypeslib.as_array(out.vals, shape=(n,)).copy() if n else np.zeros(0, np.float64)
+    finally:
+        L.ptc_tensor_free(C.byref(out))
+    return idx, vals, st.as_dict()
+
+
+def contract_coo(ca: Coo, cb: Optional[Coo], c: int, a_modes, b_modes=None, **opt):
+    """Lower-level call on prepared ``Coo`` descriptors (host or device).  Returns the raw output
+    ``Tensor`` (free with :func:`free`) and the stats dict."""
+    L = lib()
+    am = np.ascontiguousarray(a_modes, dtype=np.uint32)
+    bm = am if b_modes is None else np.ascontiguousarray(b_modes, dtype=np.uint32)
+    o = options(**opt)
+    out = Tensor()
+    st = Stats()
+    rc = L.ptc_contract(C.byref(ca), None if cb is None else C.byref(cb), c, am.ctypes.data, bm.ctypes.data,
+                        C.byref(o), C.byref(out), C.byref(st))
+    _check(rc)
+    return out, st.as_dict()
+
+
+def free(t: Tensor) -> None:
+    lib().ptc_tensor_free(C.byref(t))
+
+
+def device_count() -> int:
+    return int(lib().ptc_device_count())

@@ -1,0 +1,180 @@
+// Build-side kernels: key linearization, gathers, index tuples, panel split of the fibers.
+#include "ptc_build.cuh"
+
+namespace ptc {
+
+// One thread per nonzero: range-check every index (the reference trusts its input; an index
+// beyond its mode would corrupt the keys) and linearize the two mode tuples.
+__global__ void pack_keys_kernel(const uint32_t* __restrict__ idx, uint64_t nnz, DimSpec dims, KeySpec k1,
+                                 KeySpec k2, uint64_t* __restrict__ key1, uint64_t* __restrict__ key2,
+                                 uint32_t* __restrict__ err, bool vec4) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nnz) return;
+    const uint32_t d = dims.order;
+    const uint32_t* row = idx + i * d;
+    uint32_t v[kMaxOrder];
+    bool bad = false;
+    if (vec4) {
+        const uint4 q = *reinterpret_cast<const uint4*>(row);
+        v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+    } else {
+        for (uint32_t m = 0; m < d; ++m) v[m] = row[m];
+    }
+    for (uint32_t m = 0; m < d; ++m) bad |= v[m] >= dims.dim[m];
+    if (bad) {
+        atomicOr(err, 1u);
+        return;
+    }
+    uint64_t a = 0, b = 0;
+    for (uint32_t j = 0; j < k1.n; ++j) a += (uint64_t)v[k1.mode[j]] * k1.stride[j];
+    for (uint32_t j = 0; j < k2.n; ++j) b += (uint64_t)v[k2.mode[j]] * k2.stride[j];
+    if (key1) key1[i] = a;
+    if (key2) key2[i] = b;
+}
+
+void launch_pack_keys(const uint32_t* idx, uint64_t nnz, const DimSpec& dims, const KeySpec& k1, const KeySpec& k2,
+                      uint64_t* key1, uint64_t* key2, uint32_t* err, cudaStream_t st) {
+    if (nnz == 0) return;
+    const bool vec4 = dims.order == 4 && (reinterpret_cast<uintptr_t>(idx) & 15u) == 0;
+    pack_keys_kernel<<<ceil_div_u32(nnz, 256), 256, 0, st>>>(idx, nnz, dims, k1, k2, key1, key2, err, vec4);
+    count_launch();
+    PTC_CHECK_LAUNCH();
+}
+
+__global__ void iota_kernel(uint32_t* __restrict__ out, uint64_t n) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (uint32_t)i;
+}
+
+void launch_iota(uint32_t* out, uint64_t n, cudaStream_t st) {
+    if (n == 0) return;
+    iota_kernel<<<ceil_div_u32(n, 256), 256, 0, st>>>(out, n);
+    count_launch();
+    PTC_CHECK_LAUNCH();
+}
+
+// dst[perm[i]] = src[i]
+__global__ void scatter_u32_kernel(const uint32_t* __restrict__ src, const uint32_t* __restrict__ perm, uint64_t n,
+                                   uint32_t* __restrict__ dst) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[perm[i]] = src[i];
+}
+
+void launch_scatter_u32(const uint32_t* src, const uint32_t* perm, uint64_t n, uint32_t* dst, cudaStream_t st) {
+    if (n == 0) return;
+    scatter_u32_kernel<<<ceil_div_u32(n, 256), 256, 0, st>>>(src, perm, n, dst);
+    count_launch();
+    PTC_CHECK_LAUNCH();
+}
+
+template <typename T>
+__global__ void gather_kernel(const T* __restrict__ src, const uint32_t* __restrict__ perm, uint64_t n,
+                              T* __restrict__ dst) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = src[perm[i]];
+}
+
+template <typename T>
+void launch_gather(const T* src, const uint32_t* perm, uint64_t n, T* dst, cudaStream_t st) {
+    if (n == 0) return;
+    gather_kernel<T><<<ceil_div_u32(n, 256), 256, 0, st>>>(src, perm, n, dst);
+    count_launch();
+    PTC_CHECK_LAUNCH();
+}
+template void launch_gather<uint32_t>(const uint32_t*, const uint32_t*, uint64_t, uint32_t*, cudaStream_t);
+template void launch_gather<uint64_t>(const uint64_t*, const uint32_t*, uint64_t, uint64_t*, cudaStream_t);
+template void launch_gather<double>(const double*, const uint32_t*, uint64_t, double*, cudaStream_t);
+
+// composite[i] = key_hi[i] * radix + lo[i]
+__global__ void composite_kernel(const uint64_t* __restrict__ hi, const uint32_t* __restrict__ lo, uint64_t radix,
+                                 uint64_t n, uint64_t* __restrict__ out) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = hi[i] * radix + lo[i];
+}
+
+void launch_composite(const uint64_t* hi, const uint32_t* lo, uint64_t radix, uint64_t n, uint64_t* out,
+                      cudaStream_t st) {
+    if (n == 0) return;
+    composite_kernel<<<ceil_div_u32(n, 256), 256, 0, st>>>(hi, lo, radix, n, out);
+    count_launch();
+    PTC_CHECK_LAUNCH();
+}
+
+// tuple[r * nm + j] = idx[src[r] * order + mode[j]] for every run r (src = a representative
+// nonzero of the run, in original numbering).
+__global__ void tuples_kernel(const uint32_t* __restrict__ idx, uint32_t order, const uint32_t* __restrict__ run_start,
+                              const uint32_t* __restrict__ perm, uint64_t nruns, KeySpec ks,
+                              uint32_t* __restrict__ tuple) {
+    const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nruns) return;
+    const uint64_t src = perm[run_start[r]];
+    for (uint32_t j = 0; j < ks.n; ++j) tuple[r * ks.n + j] = idx[src * order + ks.mode[j]];
+}
+
+void launch_tuples(const uint32_t* idx, uint32_t order, const uint32_t* run_start, const uint32_t* perm, uint64_t nruns,
+                   const KeySpec& ks, uint32_t* tuple, cudaStream_t st) {
+    if (nruns == 0 || ks.n == 0) return;
+    tuples_kernel<<<ceil_div_u32(nruns, 256), 256, 0, st>>>(idx, order, run_start, perm, nruns, ks, tuple);
+    count_launch();
+    PTC_CHECK_LAUNCH();
+}
+
+// Per A nonzero (row-sorted): length of its matching fiber (0 if none).
+__global__ void fiber_len_kernel(const int32_t* __restrict__ a_fib, const uint32_t* __restrict__ fib_start, uint64_t n,
+                                 uint64_t* __restrict__ len) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int32_t f = a_fib[i];
+    len[i] = f >= 0 ? (uint64_t)(fib_start[f + 1] - fib_start[f]) : 0ull;
+}
+
+void launch_fiber_len(const int32_t* a_fib, const uint32_t* fib_start, uint64_t n, uint64_t* len, cudaStream_t st) {
+    if (n == 0) return;
+    fiber_len_kernel<<<ceil_div_u32(n, 256), 256, 0, st>>>(a_fib, fib_start, n, len);
+    count_launch();
+    PTC_CHECK_LAUNCH();
+}
+
+// Per row: flops = poff[row_end] - poff[row_start].
+__global__ void row_flops_kernel(const uint64_t* __restrict__ poff, const uint32_t* __restrict__ row_start,
+                                 uint64_t nrows, uint64_t* __restrict__ flops) {
+    const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < nrows) flops[r] = poff[row_start[r + 1]] - poff[row_start[r]];
+}
+
+void launch_row_flops(const uint64_t* poff, const uint32_t* row_start, uint64_t nrows, uint64_t* flops,
+                      cudaStream_t st) {
+    if (nrows == 0) return;
+    row_flops_kernel<<<ceil_div_u32(nrows, 256), 256, 0, st>>>(poff, row_start, nrows, flops);
+    count_launch();
+    PTC_CHECK_LAUNCH();
+}
+
+// Dense-panel split of every fiber (B sorted by fiber, then column):
+// off[f * (P + 1) + p] = first entry j of fiber f with b_col[j] >= p << log2w (fiber end if none).
+// One thread per B entry writes the panel boundaries that fall just before it; the last entry of
+// a fiber also writes the boundaries past its column.
+__global__ void panel_offsets_kernel(const uint32_t* __restrict__ b_col, const uint32_t* __restrict__ b_fib,
+                                     const uint32_t* __restrict__ fib_start, uint64_t nb, uint32_t P,
+                                     uint32_t log2w, uint32_t* __restrict__ off) {
+    const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nb) return;
+    const uint32_t f = b_fib[j];
+    const uint32_t fs = fib_start[f], fe = fib_start[f + 1];
+    const uint32_t q = b_col[j] >> log2w;
+    const int64_t qprev = (j == fs) ? -1 : (int64_t)(b_col[j - 1] >> log2w);
+    uint32_t* o = off + (uint64_t)f * (P + 1);
+    for (int64_t p = qprev + 1; p <= (int64_t)q; ++p) o[p] = (uint32_t)j;
+    if (j + 1 == fe)
+        for (uint32_t p = q + 1; p <= P; ++p) o[p] = fe;
+}
+
+void launch_panel_offsets(const uint32_t* b_col, const uint32_t* b_fib, const uint32_t* fib_start, uint64_t nb,
+                          uint32_t P, uint32_t log2w, uint32_t* off, cudaStream_t st) {
+    if (nb == 0) return;
+    panel_offsets_kernel<<<ceil_div_u32(nb, 256), 256, 0, st>>>(b_col, b_fib, fib_start, nb, P, log2w, off);
+    count_launch();
+    PTC_CHECK_LAUNCH();
+}
+
+}  // namespace ptc

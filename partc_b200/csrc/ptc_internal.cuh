@@ -1,0 +1,81 @@
+// Internal data layout shared by the build, accumulator and host-orchestration files.
+#pragma once
+
+#include "ptc_common.cuh"
+#include "ptc_cuckoo.cuh"
+
+namespace ptc {
+
+constexpr int kMaxOrder = 16;
+
+// Mixed-radix linearization of a mode tuple: key = sum_j idx[mode[j]] * stride[j], first listed
+// mode most significant.  Replaces the reference's per-mode key loops and fastmod bucket
+// arithmetic (fksCuckoo.hpp:66-94,658-672; fastmod.h:76-85) with one 64-bit key per nonzero.
+struct KeySpec {
+    uint32_t n = 0;
+    uint32_t mode[kMaxOrder] = {};
+    uint64_t stride[kMaxOrder] = {};
+    uint64_t space = 1;  // product of the mode sizes
+};
+
+struct DimSpec {
+    uint32_t order = 0;
+    uint32_t dim[kMaxOrder] = {};
+};
+
+// Device view of the grouped operands (all arrays in HBM).
+//   A side, sorted by row (A free key), COO input order kept inside a row:
+//     a_val[i], a_fib[i] (B fiber id or -1), row_start[r] (nrows+1 entries)
+//   B side, sorted by (contracted key, column), so each fiber is contiguous and ordered by column:
+//     b_col[j] (dense column id = rank of B's free key), b_val[j], fib_start[f] (nfib+1)
+//   Output index tuples: row_tuple[r * fa + m], col_tuple[q * fb + m]
+struct Operands {
+    uint64_t na = 0, nb = 0, nrows = 0, ncols = 0, nfib = 0;
+    uint32_t fa = 0, fb = 0;
+    const double* a_val = nullptr;
+    const int32_t* a_fib = nullptr;
+    const uint32_t* row_start = nullptr;
+    const uint32_t* b_col = nullptr;
+    const double* b_val = nullptr;
+    const uint32_t* fib_start = nullptr;
+    const uint32_t* row_tuple = nullptr;
+    const uint32_t* col_tuple = nullptr;
+    // dense-panel split of every fiber: panel_off[f * (npanels + 1) + p] = first entry of fiber f
+    // whose column is >= p * panel_width (null when there is a single panel)
+    const uint32_t* panel_off = nullptr;
+    uint32_t npanels = 1;
+    uint32_t panel_log2 = 0;
+    // set to nonzero by a kernel that met an impossible index (a bug guard: the access is skipped)
+    uint32_t* err = nullptr;
+};
+
+// A unit of accumulator work: one row (small-row kernel) or one (row, panel) pair.
+struct WorkItem {
+    uint32_t row;
+    uint32_t panel;
+    uint32_t slot;  // index of this item's count / output offset
+    uint32_t pad;
+};
+
+// Output destination.
+struct OutputView {
+    uint32_t* idx = nullptr;   // [nnz * (fa + fb)]
+    double* val = nullptr;     // [nnz]
+    const uint64_t* item_off = nullptr;  // output offset per item slot
+};
+
+// ---- kernels launched from the host orchestration ----
+
+void launch_pack_keys(const uint32_t* idx, uint64_t nnz, const DimSpec& dims, const KeySpec& k1,
+                      const KeySpec& k2, uint64_t* key1, uint64_t* key2, uint32_t* err, cudaStream_t st);
+
+void launch_small_rows(bool numeric, const Operands& op, const WorkItem* items, uint32_t nitems,
+                       uint64_t* counts, const OutputView& out, cudaStream_t st);
+
+void launch_panel_items(bool numeric, const Operands& op, const WorkItem* items, uint32_t nitems,
+                        uint64_t* counts, const OutputView& out, uint32_t* work_counter, int num_sms,
+                        cudaStream_t st);
+
+uint32_t small_row_max_flops();
+
+}  // namespace ptc

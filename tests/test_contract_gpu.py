@@ -1,0 +1,131 @@
+"""Parity of the CUDA engine (through the C ABI) with the reference and its C restatement.
+
+Indices and nnz must be identical as sets; values must be bit-identical (the engine sums in the
+reference's order: per output entry, a left fold over the row's A nonzeros in COO input order).
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from helpers import assert_same_output, canonical, load_golden
+from partc_b200 import gen
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])
+def test_golden(engine, path):
+    t, c, modes, gi, gv = load_golden(path)
+    idx, vals, st = engine.contract(t, None, c, modes)
+    assert_same_output(idx, vals, gi, gv, bit_exact=True)
+    assert st["out_nnz"] == gi.shape[0]
+
+
+CASES = [
+    # dims, nnz, alphas, seed, values, c, modes
+    ([500, 400, 300], 50_000, [None] * 3, 0, "uniform01", 2, [0, 1, 2]),
+    ([120, 140, 900, 17], 200_000, [1.1] * 4, 21, "uniform01", 2, [0, 1, 2, 3]),
+    ([120, 140, 900, 17], 200_000, [1.1] * 4, 21, "uniform01", 2, [1, 2, 0, 3]),
+    ([2000, 900, 3000], 300_000, [None, 1.3, None], 22, "normal", 2, [0, 2, 1]),
+    ([300, 200, 100], 40_000, [None] * 3, 23, "uniform11", 1, [2, 0, 1]),
+    ([20, 30, 25, 40, 10], 60_000, [0.9] * 5, 24, "uniform01", 3, [4, 0, 2, 1, 3]),
+]
+
+
+@pytest.mark.parametrize("case", CASES, ids=[f"c{i}" for i in range(len(CASES))])
+@pytest.mark.parametrize("panel", [0, 256])
+def test_against_oracle(engine, oracle_mod, case, panel):
+    dims, nnz, alphas, seed, values, c, modes = case
+    t = gen.random_coo(dims, nnz, alphas, seed, values)
+    o = oracle_mod.contract(t, None, c, modes)
+    idx, vals, st = engine.contract(t, None, c, modes, panel_width=panel)
+    assert st["mult_adds"] == o["flops"]
+    assert st["nrows"] == o["nrows"] and st["nfibers"] == o["nfibers"]
+    assert_same_output(idx, vals, o["idx"], o["vals"], bit_exact=True)
+
+
+def test_general_two_tensors(engine, oracle_mod):
+    """A x B with different tensors and different mode positions (the reference's
+    tc_fksCuckoo signature takes two tensors)."""
+    A = gen.random_coo([40, 300, 50], 30_000, [None, 1.1, None], 31, "uniform01")
+    B = gen.random_coo([50, 60, 40, 8], 40_000, [None, 1.0, None, None], 32, "uniform11")
+    # contract A's modes (0, 2) with B's modes (2, 0); free: A mode 1, B modes 1, 3
+    o = oracle_mod.contract(A, B, 2, [0, 2, 1], [2, 0, 3, 1])
+    idx, vals, st = engine.contract(A, B, 2, [0, 2, 1], [2, 0, 3, 1])
+    assert_same_output(idx, vals, o["idx"], o["vals"], bit_exact=True)
+
+
+def test_output_is_canonical_for_panel_rows(engine, oracle_mod):
+    """Rows come out in increasing free-key order; panel rows in increasing column order."""
+    t = gen.random_coo([50, 40, 3000], 100_000, [None, None, 1.0], 33, "uniform01")
+    idx, vals, st = engine.contract(t, None, 2, [0, 1, 2], panel_width=1024)
+    ci, cv = canonical(idx, vals)
+    # every row's entries are contiguous in the engine's output
+    rows = idx[:, 0]
+    changes = np.count_nonzero(np.diff(rows.astype(np.int64)) != 0) + 1
+    assert changes == np.unique(rows).size
+
+
+def test_device_output_and_inputs(engine, oracle_mod):
+    import torch
+    t = gen.random_coo([100, 80, 60], 20_000, [None] * 3, 34, "uniform01")
+    o = oracle_mod.contract(t, None, 2, [0, 1, 2])
+    di = torch.from_numpy(t.idx.astype(np.int32)).cuda()
+    dv = torch.from_numpy(t.vals).cuda()
+    keep = []
+    ca = engine.device_coo(di.data_ptr(), dv.data_ptr(), t.nnz, t.dims, keep)
+    out, st = engine.contract_coo(ca, None, 2, [0, 1, 2], output_location="device")
+    try:
+        n, d = out.nnz, out.order
+        idx = _wrap(out.idx, n * d, torch.int32).cpu().numpy().astype(np.uint32).reshape(n, d)
+        vals = _wrap(out.vals, n, torch.float64).cpu().numpy()
+    finally:
+        engine.free(out)
+    assert_same_output(idx, vals, o["idx"], o["vals"], bit_exact=True)
+
+
+def _wrap(ptr, n, dtype):
+    """A torch view of n elements at a raw device pointer."""
+    import ctypes
+
+    import torch
+    addr = ctypes.cast(ptr, ctypes.c_void_p).value
+
+    class _CAI:
+        __cuda_array_interface__ = {
+            "shape": (n,), "typestr": {torch.int32: "<i4", torch.float64: "<f8"}[dtype],
+            "data": (addr, False), "version": 3, "strides": None,
+        }
+    return torch.as_tensor(_CAI(), device="cuda")
+
+
+def test_error_empty_contraction(engine):
+    # contracted keys of A never meet a fiber of B
+    A = gen.random_coo([10, 10, 10], 50, [None] * 3, 35, "uniform01")
+    B = gen.CooTensor(idx=A.idx.copy(), vals=A.vals.copy(), dims=A.dims.copy())
+    A.idx[:, 0] = 0
+    B.idx[:, 0] = 1
+    B.idx[:, 2] = np.arange(B.nnz) % 10  # keep B free of accidental duplicates of A
+    with pytest.raises(engine.PtcError) as e:
+        engine.contract(A, B, 1, [0, 1, 2], [0, 1, 2])
+    assert e.value.name == "PTC_ERR_EMPTY_CONTRACTION"
+
+
+def test_error_index_range(engine):
+    t = gen.random_coo([10, 10, 10], 200, [None] * 3, 36, "uniform01")
+    bad = gen.CooTensor(idx=t.idx.copy(), vals=t.vals, dims=t.dims)
+    bad.idx[17, 2] = 10
+    with pytest.raises(engine.PtcError) as e:
+        engine.contract(bad, None, 2, [0, 1, 2])
+    assert e.value.name == "PTC_ERR_INDEX_RANGE"
+
+
+def test_repeatable(engine):
+    t = gen.random_coo([120, 140, 900, 17], 100_000, [1.1] * 4, 37, "uniform01")
+    a = engine.contract(t, None, 2, [0, 1, 2, 3])
+    b = engine.contract(t, None, 2, [0, 1, 2, 3])
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1].view(np.uint64), b[1].view(np.uint64))
