@@ -85,7 +85,8 @@ typedef struct ptc_options {
     uint32_t path;             /* PTC_PATH_TWO_PHASE (default) or PTC_PATH_LEARNED */
     uint32_t output_location;  /* PTC_HOST (default, like the reference) or PTC_DEVICE */
     uint32_t verbose;          /* 1: print the reference's stdout lines (timings, nnz) */
-    uint32_t panel_width;      /* columns per dense accumulator panel; 0 = automatic */
+    uint32_t panel_width;      /* columns per fine panel (power of two in [256, 4096]); large
+                                  rows are cut at panel boundaries into parts; 0 = automatic */
     uint64_t hash_seed;        /* seed of the cuckoo hash family */
     const ptc_sizer* sizer;    /* PTC_PATH_LEARNED: trained sizer (NULL = built-in weights) */
     uint32_t sort_rows;        /* 1: rows of the output in increasing free-key order and every
@@ -109,8 +110,11 @@ typedef struct ptc_stats {
                                   "Total time for tensor contraction") */
     double t_d2h_ms;           /* device-to-host output copies */
     uint32_t hash_attempts;    /* cuckoo builds tried (1 = first seed worked) */
-    uint32_t panel_width;      /* dense panel width used */
-    uint64_t rows_small, rows_hash, rows_panel, rows_long; /* rows per accumulator bin */
+    uint32_t panel_width;      /* fine panel width used */
+    uint64_t rows_small;       /* rows on the one-warp accumulator */
+    uint64_t rows_hash;        /* rows on the block hash accumulator */
+    uint64_t hash_parts;       /* parts those rows were cut into */
+    uint64_t rows_long;        /* rows on the sort-based accumulator */
     uint64_t rerun_rows;       /* learned path: rows rerun exactly after an overflow */
     double sizer_mean_abs_log2_err; /* learned path: mean |log2(pred/actual)| over rows */
     uint64_t kernel_launches;  /* kernels this call launched */

@@ -62,7 +62,7 @@ class Stats(C.Structure):
                 ("t_total_ms", C.c_double), ("t_h2d_ms", C.c_double), ("t_build_ms", C.c_double),
                 ("t_symbolic_ms", C.c_double), ("t_numeric_ms", C.c_double), ("t_d2h_ms", C.c_double),
                 ("hash_attempts", C.c_uint32), ("panel_width", C.c_uint32),
-                ("rows_small", C.c_uint64), ("rows_hash", C.c_uint64), ("rows_panel", C.c_uint64),
+                ("rows_small", C.c_uint64), ("rows_hash", C.c_uint64), ("hash_parts", C.c_uint64),
                 ("rows_long", C.c_uint64), ("rerun_rows", C.c_uint64), ("sizer_mean_abs_log2_err", C.c_double),
                 ("kernel_launches", C.c_uint64), ("reserved", C.c_double * 4)]
 

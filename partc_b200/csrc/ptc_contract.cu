@@ -17,6 +17,7 @@
 #include "ptc_build.cuh"
 #include "ptc_internal.cuh"
 #include "ptc_prims.cuh"
+#include "ptc_spa.cuh"
 
 namespace ptc {
 
@@ -94,6 +95,20 @@ cudaStream_t default_stream_for_thread(int device) {
         dev = device;
     }
     return st;
+}
+
+// Keep freed stream-ordered allocations in the device's pool (instead of returning them to the
+// driver at every synchronization), so repeated calls do not remap their buffers.
+void keep_pool_memory(int device) {
+    static std::mutex mu;
+    static uint64_t done = 0;  // bit per device
+    std::lock_guard<std::mutex> lock(mu);
+    if (device < 64 && (done >> device) & 1ull) return;
+    cudaMemPool_t pool;
+    PTC_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t threshold = UINT64_MAX;
+    PTC_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+    if (device < 64) done |= 1ull << device;
 }
 
 int device_sm_count(int device) {
@@ -213,9 +228,9 @@ void contract_impl(const ptc_coo* A, const ptc_coo* Bin, uint32_t c, const uint3
     if (self) PTC_REQUIRE(A->nnz > 1, PTC_ERR_TOO_FEW_NONZEROS, "Tensor B has at most one nonzeros");
     PTC_REQUIRE(opt.output_location == PTC_HOST || opt.output_location == PTC_DEVICE, PTC_ERR_INVALID_ARGUMENT,
                 "bad output_location");
-    PTC_REQUIRE(opt.panel_width == 0 || (opt.panel_width >= 256 && opt.panel_width <= 16384 &&
+    PTC_REQUIRE(opt.panel_width == 0 || (opt.panel_width >= 256 && opt.panel_width <= 4096 &&
                                          (opt.panel_width & (opt.panel_width - 1)) == 0),
-                PTC_ERR_INVALID_ARGUMENT, "panel_width must be 0 or a power of two in [256, 16384]");
+                PTC_ERR_INVALID_ARGUMENT, "panel_width must be 0 or a power of two in [256, 4096]");
 
     // device
     int ndev = 0;
@@ -230,6 +245,7 @@ void contract_impl(const ptc_coo* A, const ptc_coo* Bin, uint32_t c, const uint3
     int major = 0;
     PTC_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
     if (major != 10) throw Error{PTC_ERR_NO_DEVICE, "this library is built for sm_100a (B200) only"};
+    keep_pool_memory(device);
     cudaStream_t st = opt.stream ? static_cast<cudaStream_t>(opt.stream) : default_stream_for_thread(device);
     const int num_sms = device_sm_count(device);
 
@@ -338,45 +354,20 @@ void contract_impl(const ptc_coo* A, const ptc_coo* Bin, uint32_t c, const uint3
     stats.nfibers = nfib;
     PTC_REQUIRE(flops > 0, PTC_ERR_EMPTY_CONTRACTION, "tensor contraction not possible!! (no matching fibers)");
 
-    uint32_t W = opt.panel_width;
-    if (W == 0) {
-        W = 256;
-        while (W < ncols && W < 8192) W <<= 1;
-    }
+    // fine column panels: B fibers are split at multiples of W so a row can be cut into parts
+    // that each fit one shared-memory table (W <= table capacity, so a part always fits)
+    PTC_REQUIRE(ncols <= sym_bitmap_max_cols(), PTC_ERR_INVALID_ARGUMENT,
+                "more than 1.5M distinct B free keys is not supported yet");
+    uint32_t W = opt.panel_width ? opt.panel_width : 4096;
+    PTC_REQUIRE(W <= hash_part_capacity(), PTC_ERR_INVALID_ARGUMENT, "panel_width larger than a hash part");
     const uint32_t log2w = floor_log2(W);
-    const uint32_t P = (uint32_t)((ncols + W - 1) / W);
+    const uint32_t P = (uint32_t)std::max<uint64_t>(1, (ncols + W - 1) / W);
     stats.panel_width = W;
     uint32_t* panel_off = nullptr;
     if (P > 1) {
         panel_off = ar.alloc<uint32_t>(nfib * (uint64_t)(P + 1));
         launch_panel_offsets(b_col, b_fib, fib_start, nb, P, log2w, panel_off, st);
     }
-
-    // work items; slots in canonical (row, panel) order so the output is row-major
-    std::vector<WorkItem> small_items, panel_items;
-    uint32_t nslots = 0;
-    const uint64_t small_max = small_row_max_flops();
-    for (uint64_t r = 0; r < nrows; ++r) {
-        const uint64_t f = h_flops[r];
-        if (f == 0) continue;  // fksCuckooTC.hpp:183
-        if (f <= small_max) {
-            small_items.push_back(WorkItem{(uint32_t)r, 0, nslots++, 0});
-        } else {
-            for (uint32_t p = 0; p < P; ++p) panel_items.push_back(WorkItem{(uint32_t)r, p, nslots++, 0});
-        }
-    }
-    stats.rows_small = small_items.size();
-    stats.rows_panel = panel_items.size() / std::max(P, 1u);
-    // largest rows first (their panels are the longest work items)
-    std::stable_sort(panel_items.begin(), panel_items.end(),
-                     [&](const WorkItem& x, const WorkItem& y) { return h_flops[x.row] > h_flops[y.row]; });
-    WorkItem* d_items = ar.alloc<WorkItem>(small_items.size() + panel_items.size());
-    if (!small_items.empty())
-        PTC_CUDA(cudaMemcpyAsync(d_items, small_items.data(), small_items.size() * sizeof(WorkItem),
-                                 cudaMemcpyHostToDevice, st));
-    if (!panel_items.empty())
-        PTC_CUDA(cudaMemcpyAsync(d_items + small_items.size(), panel_items.data(),
-                                 panel_items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice, st));
 
     Operands op;
     op.na = na; op.nb = nb; op.nrows = nrows; op.ncols = ncols; op.nfib = nfib;
@@ -387,27 +378,64 @@ void contract_impl(const ptc_coo* A, const ptc_coo* Bin, uint32_t c, const uint3
     op.panel_off = panel_off; op.npanels = P; op.panel_log2 = log2w;
     op.err = err;
 
-    uint64_t* counts = ar.alloc<uint64_t>((uint64_t)nslots + 1);
+    // row classes and work lists (largest rows first)
+    uint32_t* small_flag = ar.alloc<uint32_t>(nrows + 1);
+    uint32_t* big_flag = ar.alloc<uint32_t>(nrows + 1);
+    launch_classify_rows(row_flops, nrows, small_row_max_flops(), small_flag, big_flag, st);
+    uint32_t* small_pos = ar.alloc<uint32_t>(nrows + 1);
+    uint32_t* big_pos = ar.alloc<uint32_t>(nrows + 1);
+    exclusive_scan<uint32_t>(small_flag, small_pos, nrows, ar);
+    exclusive_scan<uint32_t>(big_flag, big_pos, nrows, ar);
+    const uint32_t n_small = read_scalar(small_pos + nrows, st);
+    const uint32_t n_big = read_scalar(big_pos + nrows, st);
+    uint32_t* small_rows = ar.alloc<uint32_t>(n_small);
+    uint32_t* big_rows = ar.alloc<uint32_t>(n_big);
+    launch_compact_indices(small_flag, small_pos, nrows, small_rows, st);
+    launch_compact_indices(big_flag, big_pos, nrows, big_rows, st);
+    if (n_big > 1) {
+        uint64_t* wkey = ar.alloc<uint64_t>(n_big);
+        launch_work_keys(big_rows, n_big, row_flops, wkey, st);
+        radix_sort_pairs(wkey, big_rows, n_big, 0, 40, ar);
+    }
+    stats.rows_small = n_small;
+    stats.rows_hash = n_big;
+
+    // symbolic: exact output nnz per row (and per fine panel for the large rows)
+    uint64_t* row_d = ar.alloc<uint64_t>(nrows + 1);
+    PTC_CUDA(cudaMemsetAsync(row_d, 0, (nrows + 1) * sizeof(uint64_t), st));
+    uint32_t* panel_cnt = ar.alloc<uint32_t>((uint64_t)n_big * P);
     uint32_t* work_counter = ar.alloc<uint32_t>(1);
     OutputView none;
-    launch_small_rows(false, op, d_items, (uint32_t)small_items.size(), counts, none, st);
-    launch_panel_items(false, op, d_items + small_items.size(), (uint32_t)panel_items.size(), counts, none,
-                       work_counter, num_sms, st);
-    exclusive_scan<uint64_t>(counts, counts, nslots, ar);
-    const uint64_t out_nnz = read_scalar(counts + nslots, st);
+    launch_small_rows(false, op, small_rows, n_small, row_d, nullptr, none, st);
+    launch_sym_bitmap(op, big_rows, n_big, panel_cnt, row_d, work_counter, num_sms, st);
+    uint64_t* row_off = ar.alloc<uint64_t>(nrows + 1);
+    exclusive_scan<uint64_t>(row_d, row_off, nrows, ar);
+    const uint64_t out_nnz = read_scalar(row_off + nrows, st);
+
+    // split large rows into parts that fit a shared-memory table
+    uint32_t* nparts = ar.alloc<uint32_t>((uint64_t)n_big + 1);
+    launch_count_parts(panel_cnt, n_big, P, hash_part_capacity(), nparts, err, st);
+    exclusive_scan<uint32_t>(nparts, nparts, n_big, ar);
+    const uint32_t n_parts = read_scalar(nparts + n_big, st);
+    PTC_REQUIRE(read_scalar(err, st) == 0, PTC_ERR_INTERNAL, "a fine panel exceeds the hash part capacity");
+    PartItem* parts = ar.alloc<PartItem>(n_parts);
+    launch_fill_parts(big_rows, panel_cnt, n_big, P, hash_part_capacity(), nparts, row_off, parts, st);
+    stats.hash_parts = n_parts;
     PTC_CUDA(cudaEventRecord(ev.ev[EV_SYM], st));
 
     // ---- numeric ----
     const uint32_t od = fa + fb;
     OutputView ov;
-    ov.item_off = counts;
     PTC_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&ov.idx), std::max<uint64_t>(out_nnz * od, 1) * sizeof(uint32_t), st));
     PTC_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&ov.val), std::max<uint64_t>(out_nnz, 1) * sizeof(double), st));
-    launch_small_rows(true, op, d_items, (uint32_t)small_items.size(), nullptr, ov, st);
-    launch_panel_items(true, op, d_items + small_items.size(), (uint32_t)panel_items.size(), nullptr, ov,
-                       work_counter, num_sms, st);
+    launch_small_rows(true, op, small_rows, n_small, nullptr, row_off, ov, st);
+    launch_hash_parts(op, parts, n_parts, ov, work_counter, err, num_sms, st);
     PTC_CUDA(cudaEventRecord(ev.ev[EV_NUM], st));
-    PTC_REQUIRE(read_scalar(err, st) == 0, PTC_ERR_INTERNAL, "an accumulator kernel met an out-of-range column");
+    if (read_scalar(err, st) != 0) {
+        cudaFreeAsync(ov.idx, st);
+        cudaFreeAsync(ov.val, st);
+        throw Error{PTC_ERR_INTERNAL, "an accumulator table overflowed or met an out-of-range column"};
+    }
 
     // ---- output ----
     out->order = od;

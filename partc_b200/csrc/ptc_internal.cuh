@@ -49,33 +49,23 @@ struct Operands {
     uint32_t* err = nullptr;
 };
 
-// A unit of accumulator work: one row (small-row kernel) or one (row, panel) pair.
-struct WorkItem {
+// A part of a row for the hash accumulator: the row's columns in fine panels [p0, p1), and
+// where its output entries start.
+struct PartItem {
     uint32_t row;
-    uint32_t panel;
-    uint32_t slot;  // index of this item's count / output offset
+    uint32_t p0;
+    uint32_t p1;
     uint32_t pad;
+    uint64_t out_off;
 };
 
 // Output destination.
 struct OutputView {
     uint32_t* idx = nullptr;   // [nnz * (fa + fb)]
     double* val = nullptr;     // [nnz]
-    const uint64_t* item_off = nullptr;  // output offset per item slot
 };
-
-// ---- kernels launched from the host orchestration ----
 
 void launch_pack_keys(const uint32_t* idx, uint64_t nnz, const DimSpec& dims, const KeySpec& k1,
                       const KeySpec& k2, uint64_t* key1, uint64_t* key2, uint32_t* err, cudaStream_t st);
-
-void launch_small_rows(bool numeric, const Operands& op, const WorkItem* items, uint32_t nitems,
-                       uint64_t* counts, const OutputView& out, cudaStream_t st);
-
-void launch_panel_items(bool numeric, const Operands& op, const WorkItem* items, uint32_t nitems,
-                        uint64_t* counts, const OutputView& out, uint32_t* work_counter, int num_sms,
-                        cudaStream_t st);
-
-uint32_t small_row_max_flops();
 
 }  // namespace ptc

@@ -1,17 +1,17 @@
 // Sparse accumulators of the contraction (the reference's numeric pass, fksCuckooTC.hpp:180-357,
-// and its per-row SPA hash tables, fksCuckooSPA.hpp).
+// and its per-row SPA hash tables, fksCuckooSPA.hpp), plus the exact symbolic pass.
 //
 // Summation order.  The reference computes each output entry as a left fold over the row's A
 // nonzeros in COO input order, each term the rounded product a*b (fksCuckooTC.hpp:294-337;
-// Aux_data keeps insertion order, fksCuckoo.hpp:233-255).  Both kernels below keep exactly that
+// Aux_data keeps insertion order, fksCuckoo.hpp:233-255).  The numeric kernels keep exactly that
 // order, so values are bit-identical to the reference:
-//   * the row's products are enumerated as a stream in (A nonzero, fiber entry) order;
-//   * products of one A nonzero have distinct columns (a fiber never repeats a B free key), so
-//     they may be applied concurrently;
-//   * products of different A nonzeros that hit the same column are applied in stream order --
+//   * a row's products form a stream in (A nonzero, fiber entry) order;
+//   * the products of one A nonzero have distinct columns (a fiber never repeats a B free key),
+//     so they are applied concurrently without any ordering;
+//   * products of different A nonzeros that meet in one column are applied in stream order --
 //     by rank inside a warp (match_any), or by claim rounds inside a block.
 // Products use __dmul_rn and sums __dadd_rn so nothing is contracted into an FMA.
-#include "ptc_internal.cuh"
+#include "ptc_spa.cuh"
 
 namespace ptc {
 
@@ -26,6 +26,15 @@ __device__ __forceinline__ uint32_t hash32(uint32_t x) {
     x *= 0x846ca68bu;
     x ^= x >> 16;
     return x;
+}
+
+// "no value yet" marker of an accumulator slot: a signalling-NaN payload that no product of
+// finite or NaN operands can produce (device arithmetic returns the canonical NaN)
+constexpr unsigned long long kNoValue = 0x7ff4deadbeef0001ull;
+
+__device__ __forceinline__ void accumulate(double* slot, double p) {
+    const double v = *slot;
+    *slot = (__double_as_longlong(v) == (long long)kNoValue) ? p : __dadd_rn(v, p);
 }
 
 // Write output entry o = (row's A free tuple, column's B free tuple, value).
@@ -46,21 +55,35 @@ __device__ __forceinline__ void write_entry(const Operands& op, const OutputView
     out.val[o] = v;
 }
 
+// Fiber entries of A nonzero k that fall in fine panels [p0, p1) (the whole fiber when the
+// column space is a single panel).
+__device__ __forceinline__ void part_range(const Operands& op, int32_t f, uint32_t p0, uint32_t p1, uint32_t& s,
+                                           uint32_t& e) {
+    if (op.panel_off) {
+        const uint64_t b = (uint64_t)f * (op.npanels + 1);
+        s = op.panel_off[b + p0];
+        e = op.panel_off[b + p1];
+    } else {
+        s = op.fib_start[f];
+        e = op.fib_start[f + 1];
+    }
+}
+
 // ---------------------------------------------------------------------------------------------
 // small rows: one warp per row, private open-addressing table in shared memory
 // ---------------------------------------------------------------------------------------------
 
 constexpr int kSmallWarps = 8;
-constexpr uint32_t kSmallSlots = 1024;       // per warp
-constexpr uint32_t kSmallMaxFlops = 512;     // rows with at most this many products
+constexpr uint32_t kSmallSlots = 1024;     // per warp
+constexpr uint32_t kSmallMaxFlops = 512;   // rows with at most this many products
 constexpr uint32_t kEmptyCol = 0xffffffffu;
 
 uint32_t small_row_max_flops() { return kSmallMaxFlops; }
 
 template <bool NUMERIC>
-__global__ void __launch_bounds__(kSmallWarps * 32) small_rows_kernel(Operands op, const WorkItem* __restrict__ items,
-                                                                      uint32_t nitems, uint64_t* __restrict__ counts,
-                                                                      OutputView out) {
+__global__ void __launch_bounds__(kSmallWarps * 32)
+    small_rows_kernel(Operands op, const uint32_t* __restrict__ rows, uint32_t nrows, uint64_t* __restrict__ row_d,
+                      const uint64_t* __restrict__ row_off, OutputView out) {
     extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t warp = threadIdx.x >> 5, lane = lane_id();
     uint32_t* keys = reinterpret_cast<uint32_t*>(smem) + warp * kSmallSlots;
@@ -68,9 +91,8 @@ __global__ void __launch_bounds__(kSmallWarps * 32) small_rows_kernel(Operands o
     for (uint32_t i = lane; i < kSmallSlots; i += 32) keys[i] = kEmptyCol;
     __syncwarp();
 
-    for (uint32_t item = blockIdx.x * kSmallWarps + warp; item < nitems; item += gridDim.x * kSmallWarps) {
-        const WorkItem it = items[item];
-        const uint32_t row = it.row;
+    for (uint32_t item = blockIdx.x * kSmallWarps + warp; item < nrows; item += gridDim.x * kSmallWarps) {
+        const uint32_t row = rows[item];
         const uint32_t ka = op.row_start[row], kb = op.row_start[row + 1];
         uint32_t nnew = 0;
         for (uint32_t kw = ka; kw < kb; kw += 32) {
@@ -141,7 +163,7 @@ __global__ void __launch_bounds__(kSmallWarps * 32) small_rows_kernel(Operands o
             }
         }
         // emit (numeric) or count (symbolic), resetting the table
-        uint64_t o = NUMERIC ? out.item_off[it.slot] : 0;
+        uint64_t o = NUMERIC ? row_off[row] : 0;
         for (uint32_t i = 0; i < kSmallSlots; i += 32) {
             const uint32_t sidx = i + lane;
             const uint32_t kc = keys[sidx];
@@ -151,67 +173,164 @@ __global__ void __launch_bounds__(kSmallWarps * 32) small_rows_kernel(Operands o
             keys[sidx] = kEmptyCol;
             o += __popc(mask);
         }
-        if (!NUMERIC && lane == 0) counts[it.slot] = nnew;
+        if (!NUMERIC && lane == 0) row_d[row] = nnew;
         __syncwarp();
     }
 }
 
-void launch_small_rows(bool numeric, const Operands& op, const WorkItem* items, uint32_t nitems, uint64_t* counts,
-                       const OutputView& out, cudaStream_t st) {
-    if (nitems == 0) return;
+void launch_small_rows(bool numeric, const Operands& op, const uint32_t* rows, uint32_t nrows, uint64_t* row_d,
+                       const uint64_t* row_off, const OutputView& out, cudaStream_t st) {
+    if (nrows == 0) return;
     const size_t smem = kSmallWarps * kSmallSlots * (sizeof(uint32_t) + (numeric ? sizeof(double) : 0));
-    const uint32_t grid = ceil_div_u32(nitems, kSmallWarps);
+    const uint32_t grid = ceil_div_u32(nrows, kSmallWarps);
     if (numeric) {
         PTC_CUDA(cudaFuncSetAttribute(small_rows_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        small_rows_kernel<true><<<grid, kSmallWarps * 32, smem, st>>>(op, items, nitems, counts, out);
+        small_rows_kernel<true><<<grid, kSmallWarps * 32, smem, st>>>(op, rows, nrows, row_d, row_off, out);
     } else {
         PTC_CUDA(cudaFuncSetAttribute(small_rows_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        small_rows_kernel<false><<<grid, kSmallWarps * 32, smem, st>>>(op, items, nitems, counts, out);
+        small_rows_kernel<false><<<grid, kSmallWarps * 32, smem, st>>>(op, rows, nrows, row_d, row_off, out);
     }
     count_launch();
     PTC_CHECK_LAUNCH();
 }
 
 // ---------------------------------------------------------------------------------------------
-// dense panels: one block per (row, column panel), dense accumulator of panel_width columns
+// exact symbolic pass for the other rows: one block per row, a bitmap over every column in
+// shared memory; the first set of a bit is a new output entry, counted per fine panel
 // ---------------------------------------------------------------------------------------------
 
-constexpr int kPanelThreads = 256;
-constexpr uint32_t kNoClaim = 0xffffffffu;
+constexpr int kSymThreads = 512;
 
-template <bool NUMERIC>
-__global__ void __launch_bounds__(kPanelThreads) panel_kernel(Operands op, const WorkItem* __restrict__ items,
-                                                              uint32_t nitems, uint64_t* __restrict__ counts,
-                                                              OutputView out, uint32_t* __restrict__ work_counter) {
+__global__ void __launch_bounds__(kSymThreads)
+    sym_bitmap_kernel(Operands op, const uint32_t* __restrict__ rows, uint32_t nrows, uint32_t* __restrict__ panel_cnt,
+                      uint64_t* __restrict__ row_d, uint32_t* __restrict__ work_counter, uint32_t nwords) {
     extern __shared__ __align__(16) unsigned char smem[];
-    const uint32_t W = 1u << op.panel_log2;
-    double* acc = reinterpret_cast<double*>(smem);                                   // [W]   numeric
-    uint32_t* claim = reinterpret_cast<uint32_t*>(smem + (NUMERIC ? 8u * W : 0u));  // [W]   numeric
-    uint8_t* flag = smem + (NUMERIC ? 12u * W : 0u);                                 // [W]
-    __shared__ double wa[kPanelThreads];
-    __shared__ uint32_t ws[kPanelThreads], wl[kPanelThreads], wscan[kPanelThreads];
-    __shared__ uint32_t tmp[kPanelThreads / 32 + 1];
+    uint32_t* bits = reinterpret_cast<uint32_t*>(smem);   // [nwords]
+    uint32_t* pc = bits + nwords;                         // [npanels]
+    __shared__ uint32_t ws[kSymThreads], wl[kSymThreads], wscan[kSymThreads];
+    __shared__ uint32_t tmp[kSymThreads / 32 + 1];
     __shared__ uint32_t s_item;
     const uint32_t t = threadIdx.x;
-
-    for (uint32_t i = t; i < W; i += kPanelThreads) {
-        flag[i] = 0;
-        if (NUMERIC) claim[i] = kNoClaim;
-    }
-    const uint32_t P1 = op.npanels + 1;
+    const uint32_t P = op.npanels;
+    for (uint32_t i = t; i < nwords; i += kSymThreads) bits[i] = 0;
+    for (uint32_t i = t; i < P; i += kSymThreads) pc[i] = 0;
 
     for (;;) {
         __syncthreads();
         if (t == 0) s_item = atomicAdd(work_counter, 1u);
         __syncthreads();
-        const uint32_t item_i = s_item;
-        if (item_i >= nitems) break;
-        const WorkItem it = items[item_i];
-        const uint32_t row = it.row, p = it.panel;
-        const uint32_t base = p << op.panel_log2;
+        const uint32_t item = s_item;
+        if (item >= nrows) break;
+        const uint32_t row = rows[item];
         const uint32_t ka = op.row_start[row], kb = op.row_start[row + 1];
+        for (uint32_t kw = ka; kw < kb; kw += kSymThreads) {
+            const uint32_t k = kw + t;
+            uint32_t L = 0, s = 0;
+            if (k < kb) {
+                const int32_t f = op.a_fib[k];
+                if (f >= 0) {
+                    s = op.fib_start[f];
+                    L = op.fib_start[f + 1] - s;
+                }
+            }
+            uint32_t total;
+            const uint32_t excl = block_exclusive_scan<uint32_t, kSymThreads>(L, tmp, &total);
+            ws[t] = s;
+            wl[t] = L;
+            wscan[t] = excl;
+            __syncthreads();
+            uint32_t kk = 0;
+            for (uint32_t p = t; p < total; p += kSymThreads) {
+                while (kk + 1 < kSymThreads && wscan[kk] + wl[kk] <= p) ++kk;
+                const uint32_t col = op.b_col[ws[kk] + (p - wscan[kk])];
+                const uint32_t bit = 1u << (col & 31);
+                const uint32_t old = atomicOr(&bits[col >> 5], bit);
+                const bool fresh = !(old & bit);
+                const uint32_t active = __activemask();
+                const uint32_t panel = fresh ? (col >> op.panel_log2) : 0xffffffffu;
+                const uint32_t m = __match_any_sync(active, panel);
+                if (fresh && (m & lanemask_lt()) == 0) atomicAdd(&pc[panel], (uint32_t)__popc(m));
+            }
+            __syncthreads();
+        }
+        uint32_t dsum = 0;
+        for (uint32_t p = t; p < P; p += kSymThreads) {
+            const uint32_t v = pc[p];
+            panel_cnt[(uint64_t)item * P + p] = v;
+            dsum += v;
+            pc[p] = 0;
+        }
+        for (uint32_t i = t; i < nwords; i += kSymThreads) bits[i] = 0;
+        dsum = warp_sum(dsum);
+        if (lane_id() == 0 && dsum) atomicAdd(reinterpret_cast<unsigned long long*>(&row_d[row]), (unsigned long long)dsum);
+    }
+}
 
-        for (uint32_t kw = ka; kw < kb; kw += kPanelThreads) {
+uint32_t sym_bitmap_max_cols() { return 1536u * 1024u; }  // 192 KiB of bitmap
+
+void launch_sym_bitmap(const Operands& op, const uint32_t* rows, uint32_t nrows, uint32_t* panel_cnt, uint64_t* row_d,
+                       uint32_t* work_counter, int num_sms, cudaStream_t st) {
+    if (nrows == 0) return;
+    const uint32_t nwords = (uint32_t)((op.ncols + 31) / 32);
+    const size_t smem = (size_t)(nwords + op.npanels) * sizeof(uint32_t);
+    PTC_CUDA(cudaMemsetAsync(work_counter, 0, sizeof(uint32_t), st));
+    PTC_CUDA(cudaFuncSetAttribute(sym_bitmap_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 1;
+    PTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sym_bitmap_kernel, kSymThreads, smem));
+    per_sm = per_sm < 1 ? 1 : per_sm;
+    const uint32_t grid = (uint32_t)std::min<uint64_t>(nrows, (uint64_t)num_sms * per_sm);
+    sym_bitmap_kernel<<<grid, kSymThreads, smem, st>>>(op, rows, nrows, panel_cnt, row_d, work_counter, nwords);
+    count_launch();
+    PTC_CHECK_LAUNCH();
+}
+
+// ---------------------------------------------------------------------------------------------
+// numeric pass for the other rows: one block per part (a row's columns in fine panels
+// [p0, p1)), open-addressing table of kHashSlots in shared memory
+// ---------------------------------------------------------------------------------------------
+
+constexpr int kHashThreads = 512;
+constexpr int kHashItems = 4;                          // products per thread per chunk
+constexpr int kChunk = kHashThreads * kHashItems;      // 2048 products
+constexpr uint32_t kHashSlots = 8192;
+constexpr uint32_t kClaimCells = 2048;
+constexpr uint32_t kNoClaim = 0xffffffffu;
+
+uint32_t hash_part_capacity() { return kHashSlots * 3 / 4; }  // load factor <= 0.75
+
+__global__ void __launch_bounds__(kHashThreads, 2)
+    hash_part_kernel(Operands op, const PartItem* __restrict__ parts, uint32_t nparts, OutputView out,
+                     uint32_t* __restrict__ work_counter, uint32_t* __restrict__ overflow) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    double* vals = reinterpret_cast<double*>(smem);                               // [kHashSlots]
+    uint32_t* keys = reinterpret_cast<uint32_t*>(vals + kHashSlots);              // [kHashSlots]
+    uint32_t* claim = keys + kHashSlots;                                          // [kClaimCells]
+    __shared__ double wa[kHashThreads];
+    __shared__ uint32_t ws[kHashThreads], wl[kHashThreads], wscan[kHashThreads];
+    __shared__ uint32_t tmp[kHashThreads / 32 + 1];
+    __shared__ uint32_t wtot[kHashThreads / 32];
+    __shared__ uint32_t s_item;
+    const uint32_t t = threadIdx.x, lane = lane_id(), warp = t >> 5;
+    constexpr uint32_t kWarps = kHashThreads / 32;
+
+    for (uint32_t i = t; i < kHashSlots; i += kHashThreads) {
+        keys[i] = kEmptyCol;
+        reinterpret_cast<unsigned long long*>(vals)[i] = kNoValue;
+    }
+    for (uint32_t i = t; i < kClaimCells; i += kHashThreads) claim[i] = kNoClaim;
+
+    for (;;) {
+        __syncthreads();
+        if (t == 0) s_item = atomicAdd(work_counter, 1u);
+        __syncthreads();
+        const uint32_t item = s_item;
+        if (item >= nparts) break;
+        const PartItem it = parts[item];
+        const uint32_t row = it.row;
+        const uint32_t ka = op.row_start[row], kb = op.row_start[row + 1];
+        bool full = false;  // table overflow (only possible with an underestimated size)
+
+        for (uint32_t kw = ka; kw < kb; kw += kHashThreads) {
             const uint32_t k = kw + t;
             uint32_t L = 0, s = 0;
             double a = 0.0;
@@ -219,124 +338,139 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(Operands op, const
                 const int32_t f = op.a_fib[k];
                 if (f >= 0) {
                     uint32_t e;
-                    if (op.panel_off) {
-                        s = op.panel_off[(uint64_t)f * P1 + p];
-                        e = op.panel_off[(uint64_t)f * P1 + p + 1];
-                    } else {
-                        s = op.fib_start[f];
-                        e = op.fib_start[f + 1];
-                    }
+                    part_range(op, f, it.p0, it.p1, s, e);
                     L = e - s;
-                    if (NUMERIC) a = op.a_val[k];
+                    a = op.a_val[k];
                 }
             }
             uint32_t total;
-            const uint32_t excl = block_exclusive_scan<uint32_t, kPanelThreads>(L, tmp, &total);
+            const uint32_t excl = block_exclusive_scan<uint32_t, kHashThreads>(L, tmp, &total);
             ws[t] = s;
             wl[t] = L;
             wscan[t] = excl;
-            if (NUMERIC) wa[t] = a;
+            wa[t] = a;
             __syncthreads();
 
-            uint32_t kcur = 0;
-            for (uint32_t c0 = 0; c0 < total; c0 += kPanelThreads) {
-                while (kcur + 1 < kPanelThreads && wscan[kcur] + wl[kcur] <= c0) ++kcur;
-                const uint32_t cend = min(c0 + kPanelThreads, total);
+            uint32_t kcur = 0;   // uniform: A nonzero holding the chunk's first product
+            uint32_t kk = 0;     // per thread cursor
+            for (uint32_t c0 = 0; c0 < total; c0 += kChunk) {
+                while (kcur + 1 < kHashThreads && wscan[kcur] + wl[kcur] <= c0) ++kcur;
+                const uint32_t cend = min(c0 + (uint32_t)kChunk, total);
                 const bool single = wscan[kcur] + wl[kcur] >= cend;
-                const uint32_t pi = c0 + t;
-                bool valid = pi < total;
-                uint32_t kk = kcur;
-                if (!single && valid) {
-                    uint32_t lo = kcur, hi = kPanelThreads;
-                    while (hi - lo > 1) {
-                        const uint32_t mid = (lo + hi) >> 1;
-                        if (wscan[mid] <= pi) lo = mid; else hi = mid;
+                uint32_t slot[kHashItems];
+                double prod[kHashItems];
+                uint32_t col[kHashItems];
+                if (kk < kcur) kk = kcur;
+#pragma unroll
+                for (int i = 0; i < kHashItems; ++i) {
+                    const uint32_t p = c0 + i * kHashThreads + t;
+                    col[i] = kEmptyCol;
+                    prod[i] = 0.0;
+                    if (p < total) {
+                        while (kk + 1 < kHashThreads && wscan[kk] + wl[kk] <= p) ++kk;
+                        const uint32_t j = ws[kk] + (p - wscan[kk]);
+                        col[i] = op.b_col[j];
+                        prod[i] = __dmul_rn(wa[kk], op.b_val[j]);
                     }
-                    kk = lo;
                 }
-                uint32_t col = 0;
-                double v = 0.0;
-                if (valid) {
-                    const uint32_t j = ws[kk] + (pi - wscan[kk]);
-                    col = op.b_col[j] - base;
-                    if (col >= W) {  // impossible for a correct panel split; never touch memory
-                        atomicOr(op.err, 1u);
-                        valid = false;
-                        col = 0;
-                    }
-                    if (NUMERIC) v = __dmul_rn(wa[kk], op.b_val[j]);
-                }
-                if (!NUMERIC) {
-                    if (valid) flag[col] = 1;
-                } else if (single) {
-                    if (valid) {
-                        if (flag[col]) acc[col] = __dadd_rn(acc[col], v);
-                        else { acc[col] = v; flag[col] = 1; }
-                    }
-                    __syncthreads();
-                } else {
-                    // several A nonzeros in this chunk: apply per column in stream order
-                    bool pending = valid;
-                    for (;;) {
-                        if (pending) atomicMin(&claim[col], t);
-                        __syncthreads();
-                        const bool mine = pending && claim[col] == t;
-                        __syncthreads();
-                        if (mine) {
-                            if (flag[col]) acc[col] = __dadd_rn(acc[col], v);
-                            else { acc[col] = v; flag[col] = 1; }
-                            claim[col] = kNoClaim;
-                            pending = false;
+                // find or insert every product's column (concurrent inserts of distinct keys are safe)
+#pragma unroll
+                for (int i = 0; i < kHashItems; ++i) {
+                    slot[i] = kEmptyCol;
+                    if (col[i] != kEmptyCol) {
+                        uint32_t h = hash32(col[i]) & (kHashSlots - 1);
+                        for (uint32_t probe = 0; probe < kHashSlots; ++probe) {
+                            const uint32_t cur = keys[h];
+                            if (cur == col[i]) { slot[i] = h; break; }
+                            if (cur == kEmptyCol) {
+                                const uint32_t old = atomicCAS(&keys[h], kEmptyCol, col[i]);
+                                if (old == kEmptyCol || old == col[i]) { slot[i] = h; break; }
+                            }
+                            h = (h + 1) & (kHashSlots - 1);
                         }
-                        if (!__syncthreads_or(pending)) break;
+                        if (slot[i] == kEmptyCol) { full = true; col[i] = kEmptyCol; }
+                    }
+                }
+                if (single) {
+                    // one A nonzero: every column distinct, no ordering needed
+#pragma unroll
+                    for (int i = 0; i < kHashItems; ++i)
+                        if (col[i] != kEmptyCol) accumulate(&vals[slot[i]], prod[i]);
+                    // the next chunk may start another A nonzero that meets these columns
+                    const uint32_t nend = min(cend + (uint32_t)kChunk, total);
+                    const bool next_same = cend < total && wscan[kcur] + wl[kcur] >= nend;
+                    if (!next_same) __syncthreads();
+                } else {
+                    // several A nonzeros: per column, apply in stream order (claim rounds)
+                    __syncthreads();
+                    bool pending[kHashItems];
+#pragma unroll
+                    for (int i = 0; i < kHashItems; ++i) pending[i] = col[i] != kEmptyCol;
+                    for (uint32_t round = 0; round < (uint32_t)kChunk + 1; ++round) {
+#pragma unroll
+                        for (int i = 0; i < kHashItems; ++i)
+                            if (pending[i]) atomicMin(&claim[slot[i] & (kClaimCells - 1)], i * kHashThreads + t);
+                        __syncthreads();
+                        bool mine[kHashItems];
+#pragma unroll
+                        for (int i = 0; i < kHashItems; ++i)
+                            mine[i] = pending[i] && claim[slot[i] & (kClaimCells - 1)] == i * kHashThreads + t;
+                        __syncthreads();
+                        bool left = false;
+#pragma unroll
+                        for (int i = 0; i < kHashItems; ++i) {
+                            if (mine[i]) {
+                                accumulate(&vals[slot[i]], prod[i]);
+                                claim[slot[i] & (kClaimCells - 1)] = kNoClaim;
+                                pending[i] = false;
+                            }
+                            left |= pending[i];
+                        }
+                        if (!__syncthreads_or(left)) break;
                     }
                 }
             }
             __syncthreads();
         }
+        if (__syncthreads_or(full)) {
+            if (t == 0) atomicOr(overflow, 1u);
+        }
 
-        // count / emit the panel in column order, clearing it for the next item
-        const uint32_t per = W / kPanelThreads;  // W >= 256
-        const uint32_t lo = t * per;
+        // emit in slot order: warp w owns slots [w * span, (w + 1) * span)
+        constexpr uint32_t span = kHashSlots / kWarps;
         uint32_t cnt = 0;
-        for (uint32_t i = 0; i < per; ++i) cnt += flag[lo + i];
-        uint32_t total;
-        const uint32_t excl = block_exclusive_scan<uint32_t, kPanelThreads>(cnt, tmp, &total);
-        if (NUMERIC) {
-            uint64_t o = out.item_off[it.slot] + excl;
-            for (uint32_t i = 0; i < per; ++i) {
-                if (flag[lo + i]) {
-                    write_entry(op, out, o++, row, base + lo + i, acc[lo + i]);
-                    flag[lo + i] = 0;
-                }
+        for (uint32_t i = 0; i < span; i += 32)
+            cnt += __popc(__ballot_sync(kFullMask, keys[warp * span + i + lane] != kEmptyCol));
+        if (lane == 0) wtot[warp] = cnt;
+        __syncthreads();
+        uint64_t o = it.out_off;
+        for (uint32_t w = 0; w < warp; ++w) o += wtot[w];
+        for (uint32_t i = 0; i < span; i += 32) {
+            const uint32_t sidx = warp * span + i + lane;
+            const uint32_t kc = keys[sidx];
+            const bool occ = kc != kEmptyCol;
+            const uint32_t m = __ballot_sync(kFullMask, occ);
+            if (occ) {
+                write_entry(op, out, o + __popc(m & lanemask_lt()), row, kc, vals[sidx]);
+                keys[sidx] = kEmptyCol;
+                reinterpret_cast<unsigned long long*>(vals)[sidx] = kNoValue;
             }
-        } else {
-            for (uint32_t i = 0; i < per; ++i) flag[lo + i] = 0;
-            if (t == 0) counts[it.slot] = total;
+            o += __popc(m);
         }
     }
 }
 
-void launch_panel_items(bool numeric, const Operands& op, const WorkItem* items, uint32_t nitems, uint64_t* counts,
-                        const OutputView& out, uint32_t* work_counter, int num_sms, cudaStream_t st) {
-    if (nitems == 0) return;
-    const uint32_t W = 1u << op.panel_log2;
-    const size_t smem = numeric ? (size_t)13 * W : (size_t)W;
+void launch_hash_parts(const Operands& op, const PartItem* parts, uint32_t nparts, const OutputView& out,
+                       uint32_t* work_counter, uint32_t* overflow, int num_sms, cudaStream_t st) {
+    if (nparts == 0) return;
+    const size_t smem = (size_t)kHashSlots * (sizeof(double) + sizeof(uint32_t)) + kClaimCells * sizeof(uint32_t);
     PTC_CUDA(cudaMemsetAsync(work_counter, 0, sizeof(uint32_t), st));
+    PTC_CUDA(cudaFuncSetAttribute(hash_part_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 1;
-    if (numeric) {
-        PTC_CUDA(cudaFuncSetAttribute(panel_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        PTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, panel_kernel<true>, kPanelThreads, smem));
-    } else {
-        PTC_CUDA(cudaFuncSetAttribute(panel_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        PTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, panel_kernel<false>, kPanelThreads, smem));
-    }
+    PTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hash_part_kernel, kHashThreads, smem));
     per_sm = per_sm < 1 ? 1 : per_sm;
-    const uint32_t grid = (uint32_t)std::min<uint64_t>(nitems, (uint64_t)num_sms * per_sm);
-    if (numeric)
-        panel_kernel<true><<<grid, kPanelThreads, smem, st>>>(op, items, nitems, counts, out, work_counter);
-    else
-        panel_kernel<false><<<grid, kPanelThreads, smem, st>>>(op, items, nitems, counts, out, work_counter);
+    const uint32_t grid = (uint32_t)std::min<uint64_t>(nparts, (uint64_t)num_sms * per_sm);
+    hash_part_kernel<<<grid, kHashThreads, smem, st>>>(op, parts, nparts, out, work_counter, overflow);
     count_launch();
     PTC_CHECK_LAUNCH();
 }
