@@ -85,8 +85,9 @@ typedef struct ptc_options {
     uint32_t path;             /* PTC_PATH_TWO_PHASE (default) or PTC_PATH_LEARNED */
     uint32_t output_location;  /* PTC_HOST (default, like the reference) or PTC_DEVICE */
     uint32_t verbose;          /* 1: print the reference's stdout lines (timings, nnz) */
-    uint32_t panel_width;      /* columns per fine panel (power of two in [256, 4096]); large
-                                  rows are cut at panel boundaries into parts; 0 = automatic */
+    uint32_t panel_width;      /* columns per fine panel (power of two in [32, 4096]); large
+                                  rows are cut at panel boundaries into parts and each warp owns
+                                  a range of panels; 0 = automatic */
     uint64_t hash_seed;        /* seed of the cuckoo hash family */
     const ptc_sizer* sizer;    /* PTC_PATH_LEARNED: trained sizer (NULL = built-in weights) */
     uint32_t sort_rows;        /* 1: rows of the output in increasing free-key order and every
@@ -157,6 +158,57 @@ void ptc_tensor_free(ptc_tensor* t);
 
 /* Number of CUDA devices the library can use (sm_100 class). */
 int ptc_device_count(void);
+
+/* ---- learned sizer (no counterpart in the reference: it replaces the symbolic pass) ----
+ * A 16 -> 64 -> 64 -> 1 ReLU network with BF16 weights and FP32 accumulation that predicts
+ * log2(1 + output nnz) of a row from per-row features computed on the device.  It is trained
+ * and evaluated by the library's own CUDA kernels. */
+#define PTC_SIZER_FEATURES 16
+#define PTC_SIZER_PARAMS 5313 /* W1[64][16], b1[64], W2[64][64], b2[64], w3[64], b3 */
+
+typedef struct ptc_train_options {
+    uint32_t struct_size;  /* sizeof(ptc_train_options) */
+    uint32_t epochs;       /* passes over the samples (default 20) */
+    uint32_t batch;        /* samples per Adam step (default 8192) */
+    float lr;              /* Adam learning rate (default 2e-3) */
+    uint64_t seed;         /* minibatch shuffling seed */
+    int32_t device;        /* -1 = current device */
+    uint32_t reserved[5];
+} ptc_train_options;
+
+typedef struct ptc_train_stats {
+    float first_epoch_loss;  /* mean squared error (log2 units) over the first epoch */
+    float final_epoch_loss;  /* ... over the last epoch */
+    uint32_t epochs;
+    uint64_t steps;          /* Adam steps taken by this sizer so far */
+    double ms;               /* wall time of the training call */
+} ptc_train_stats;
+
+void ptc_train_options_init(ptc_train_options* opt);
+/* New sizer with seeded He-normal weights. */
+ptc_status ptc_sizer_create(uint64_t seed, ptc_sizer** out);
+ptc_status ptc_sizer_load(const char* path, ptc_sizer** out);
+ptc_status ptc_sizer_save(const ptc_sizer* s, const char* path);
+void ptc_sizer_free(ptc_sizer* s);
+/* FP32 master weights in the PTC_SIZER_PARAMS order (the device computes with BF16 copies). */
+ptc_status ptc_sizer_get_params(const ptc_sizer* s, float* params);
+ptc_status ptc_sizer_set_params(ptc_sizer* s, const float* params);
+/* Training samples of one contraction: the features and log2(1 + exact output nnz) of every
+ * row the learned path sizes.  *features (n x PTC_SIZER_FEATURES) and *targets (n) are
+ * allocated by the library; release them with ptc_buffer_free. */
+ptc_status ptc_sizer_collect(const ptc_coo* A, const ptc_coo* B, uint32_t c, const uint32_t* a_modes,
+                             const uint32_t* b_modes, const ptc_options* opt, float** features,
+                             float** targets, uint64_t* n);
+/* Adam on the mean squared error, minibatches shuffled per epoch; all math on the device. */
+ptc_status ptc_sizer_train(ptc_sizer* s, const float* features, const float* targets, uint64_t n,
+                           const ptc_train_options* opt, ptc_train_stats* stats);
+/* out[i] = predicted log2(1 + output nnz) for n feature rows (host arrays). */
+ptc_status ptc_sizer_predict(const ptc_sizer* s, const float* features, uint64_t n, int32_t device,
+                             float* out);
+/* Gradient of the mean squared error over n samples (host arrays; grads has PTC_SIZER_PARAMS). */
+ptc_status ptc_sizer_gradients(const ptc_sizer* s, const float* features, const float* targets,
+                               uint64_t n, int32_t device, float* grads, float* loss);
+void ptc_buffer_free(void* p);
 
 #ifdef __cplusplus
 }

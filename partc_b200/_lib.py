@@ -28,8 +28,12 @@ STATUS = {
 # every function include/partc.h declares (checked by the CPU tests)
 EXPORTS = [
     "ptc_options_init", "ptc_last_error", "ptc_status_string", "ptc_contract", "ptc_self_contract",
-    "ptc_tensor_free", "ptc_device_count",
+    "ptc_tensor_free", "ptc_device_count", "ptc_train_options_init", "ptc_sizer_create", "ptc_sizer_load",
+    "ptc_sizer_save", "ptc_sizer_free", "ptc_sizer_get_params", "ptc_sizer_set_params", "ptc_sizer_collect",
+    "ptc_sizer_train", "ptc_sizer_predict", "ptc_sizer_gradients", "ptc_buffer_free",
 ]
+SIZER_FEATURES = 16
+SIZER_PARAMS = 5313
 
 
 class PtcError(RuntimeError):
@@ -71,6 +75,16 @@ class Stats(C.Structure):
                 for name, _ in self._fields_ if name != "reserved"}
 
 
+class TrainOptions(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("epochs", C.c_uint32), ("batch", C.c_uint32), ("lr", C.c_float),
+                ("seed", C.c_uint64), ("device", C.c_int32), ("reserved", C.c_uint32 * 5)]
+
+
+class TrainStats(C.Structure):
+    _fields_ = [("first_epoch_loss", C.c_float), ("final_epoch_loss", C.c_float), ("epochs", C.c_uint32),
+                ("steps", C.c_uint64), ("ms", C.c_double)]
+
+
 _lib = None
 
 
@@ -95,6 +109,29 @@ def lib():
         L.ptc_tensor_free.argtypes = [C.POINTER(Tensor)]
         L.ptc_tensor_free.restype = None
         L.ptc_device_count.restype = C.c_int
+        P, F = C.POINTER, C.c_float
+        L.ptc_train_options_init.argtypes = [P(TrainOptions)]
+        L.ptc_train_options_init.restype = None
+        L.ptc_sizer_create.argtypes = [C.c_uint64, P(C.c_void_p)]
+        L.ptc_sizer_load.argtypes = [C.c_char_p, P(C.c_void_p)]
+        L.ptc_sizer_save.argtypes = [C.c_void_p, C.c_char_p]
+        L.ptc_sizer_free.argtypes = [C.c_void_p]
+        L.ptc_sizer_free.restype = None
+        L.ptc_sizer_get_params.argtypes = [C.c_void_p, C.c_void_p]
+        L.ptc_sizer_set_params.argtypes = [C.c_void_p, C.c_void_p]
+        L.ptc_sizer_collect.argtypes = [P(Coo), P(Coo), C.c_uint32, C.c_void_p, C.c_void_p, P(Options),
+                                        P(P(F)), P(P(F)), P(C.c_uint64)]
+        L.ptc_sizer_train.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, P(TrainOptions),
+                                      P(TrainStats)]
+        L.ptc_sizer_predict.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int32, C.c_void_p]
+        L.ptc_sizer_gradients.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_int32, C.c_void_p,
+                                          P(F)]
+        L.ptc_buffer_free.argtypes = [C.c_void_p]
+        L.ptc_buffer_free.restype = None
+        for name in ("ptc_sizer_create", "ptc_sizer_load", "ptc_sizer_save", "ptc_sizer_get_params",
+                     "ptc_sizer_set_params", "ptc_sizer_collect", "ptc_sizer_train", "ptc_sizer_predict",
+                     "ptc_sizer_gradients"):
+            getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
 
@@ -183,3 +220,92 @@ def free(t: Tensor) -> None:
 
 def device_count() -> int:
     return int(lib().ptc_device_count())
+
+
+# ---- learned sizer -------------------------------------------------------------------------
+
+class Sizer:
+    """Owning handle of a ptc_sizer (the learned output-size predictor)."""
+
+    def __init__(self, handle):
+        self.h = handle
+
+    @classmethod
+    def create(cls, seed: int = 0) -> "Sizer":
+        h = C.c_void_p()
+        _check(lib().ptc_sizer_create(seed, C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def load(cls, path: str) -> "Sizer":
+        h = C.c_void_p()
+        _check(lib().ptc_sizer_load(path.encode(), C.byref(h)))
+        return cls(h)
+
+    def save(self, path: str) -> None:
+        _check(lib().ptc_sizer_save(self.h, path.encode()))
+
+    def params(self) -> np.ndarray:
+        out = np.empty(SIZER_PARAMS, dtype=np.float32)
+        _check(lib().ptc_sizer_get_params(self.h, out.ctypes.data))
+        return out
+
+    def set_params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        _check(lib().ptc_sizer_set_params(self.h, p.ctypes.data))
+
+    def train(self, x: np.ndarray, t: np.ndarray, epochs=20, batch=8192, lr=2e-3, seed=7, device=-1) -> dict:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        o = TrainOptions()
+        lib().ptc_train_options_init(C.byref(o))
+        o.epochs, o.batch, o.lr, o.seed, o.device = epochs, batch, lr, seed, device
+        st = TrainStats()
+        _check(lib().ptc_sizer_train(self.h, x.ctypes.data, t.ctypes.data, len(t), C.byref(o), C.byref(st)))
+        return {"first_epoch_loss": st.first_epoch_loss, "final_epoch_loss": st.final_epoch_loss,
+                "epochs": st.epochs, "steps": st.steps, "ms": st.ms}
+
+    def predict(self, x: np.ndarray, device=-1) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        out = np.empty(x.shape[0], dtype=np.float32)
+        _check(lib().ptc_sizer_predict(self.h, x.ctypes.data, x.shape[0], device, out.ctypes.data))
+        return out
+
+    def gradients(self, x: np.ndarray, t: np.ndarray, device=-1):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        g = np.empty(SIZER_PARAMS, dtype=np.float32)
+        loss = C.c_float()
+        _check(lib().ptc_sizer_gradients(self.h, x.ctypes.data, t.ctypes.data, len(t), device, g.ctypes.data,
+                                         C.byref(loss)))
+        return float(loss.value), g
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.ptc_sizer_free(self.h)
+            self.h = None
+
+
+def sizer_collect(A, B, c, a_modes, b_modes=None, **opt):
+    """Features and log2(1 + exact output nnz) of the rows the learned path sizes."""
+    L = lib()
+    keep: list = []
+    ca = _host_coo(A, keep)
+    cb = None if B is None else _host_coo(B, keep)
+    am = np.ascontiguousarray(a_modes, dtype=np.uint32)
+    bm = am if b_modes is None else np.ascontiguousarray(b_modes, dtype=np.uint32)
+    o = options(**opt)
+    fx = C.POINTER(C.c_float)()
+    ft = C.POINTER(C.c_float)()
+    n = C.c_uint64()
+    _check(L.ptc_sizer_collect(C.byref(ca), None if cb is None else C.byref(cb), c, am.ctypes.data, bm.ctypes.data,
+                               C.byref(o), C.byref(fx), C.byref(ft), C.byref(n)))
+    try:
+        nn = n.value
+        x = np.ctypeslib.as_array(fx, shape=(max(nn, 1) * SIZER_FEATURES,))[: nn * SIZER_FEATURES].reshape(
+            nn, SIZER_FEATURES).copy()
+        t = np.ctypeslib.as_array(ft, shape=(max(nn, 1),))[:nn].copy()
+    finally:
+        L.ptc_buffer_free(C.cast(fx, C.c_void_p))
+        L.ptc_buffer_free(C.cast(ft, C.c_void_p))
+    return x, t

@@ -10,6 +10,9 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+
+#include <dlfcn.h>
+#include <sys/mman.h>
 #include <string>
 #include <vector>
 
@@ -17,6 +20,8 @@
 #include "ptc_build.cuh"
 #include "ptc_internal.cuh"
 #include "ptc_prims.cuh"
+#include "ptc_learned.cuh"
+#include "ptc_sizer.cuh"
 #include "ptc_spa.cuh"
 
 namespace ptc {
@@ -28,6 +33,13 @@ static thread_local char g_last_error_buf[512];
 void set_last_error(ptc_status, const std::string& msg) { g_last_error = msg; }
 
 namespace {
+
+// rows averaging fewer products per A nonzero than this use the sort-based accumulator
+constexpr uint32_t kEscMaxAvgProducts = 32;
+// a window of fine panels at least 1/kDenseMinFraction full becomes a dense part
+constexpr uint32_t kDenseMinFraction = 5;
+// largest product count the sort-based accumulator buffers (32 bytes per product)
+constexpr uint64_t kEscMaxProducts = 256ull << 20;
 
 KeySpec make_keyspec(const uint32_t* dims, const uint32_t* modes, uint32_t n) {
     KeySpec k;
@@ -136,6 +148,7 @@ T read_scalar(const T* dptr, cudaStream_t st) {
 struct Ranked {
     uint32_t* perm = nullptr;       // [n] original index of the i-th smallest
     uint32_t* rank_of = nullptr;    // [n] rank of original element i
+    uint32_t* run_of = nullptr;     // [n] rank of the i-th smallest
     uint32_t* run_start = nullptr;  // [nruns + 1] in sorted order
     uint64_t nruns = 0;
 };
@@ -148,11 +161,11 @@ Ranked rank_keys(const uint64_t* keys, uint64_t n, uint64_t space, Arena& ar) {
     PTC_CUDA(cudaMemcpyAsync(k, keys, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, st));
     launch_iota(r.perm, n, st);
     radix_sort_pairs(k, r.perm, n, 0, bits_for_space(space), ar);
-    uint32_t* run_of_sorted = ar.alloc<uint32_t>(n);
+    r.run_of = ar.alloc<uint32_t>(n);
     r.run_start = ar.alloc<uint32_t>(n + 1);
-    r.nruns = runs_of_sorted(k, n, run_of_sorted, r.run_start, nullptr, ar);
+    r.nruns = runs_of_sorted(k, n, r.run_of, r.run_start, nullptr, ar);
     r.rank_of = ar.alloc<uint32_t>(n);
-    launch_scatter_u32(run_of_sorted, r.perm, n, r.rank_of, st);
+    launch_scatter_u32(r.run_of, r.perm, n, r.rank_of, st);
     return r;
 }
 
@@ -184,6 +197,73 @@ DeviceCoo to_device(const ptc_coo* t, Arena& ar) {
     return d;
 }
 
+// Device -> pageable host copy of a large result: chunks go by DMA into two pinned staging
+// buffers while host threads copy the previous chunk out (and fault in the destination pages)
+// in parallel.  A plain cudaMemcpy into fresh pageable memory runs at a small fraction of this.
+class HostCopier {
+  public:
+    static constexpr size_t kStage = 128ull << 20;
+    void copy(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+        if (bytes == 0) return;
+        ensure();
+        const size_t nchunks = (bytes + kStage - 1) / kStage;
+        auto issue = [&](size_t c) {
+            const size_t off = c * kStage, n = std::min(kStage, bytes - off);
+            PTC_CUDA(cudaMemcpyAsync(stage_[c & 1], static_cast<const char*>(src) + off, n, cudaMemcpyDeviceToHost, st));
+            PTC_CUDA(cudaEventRecord(ev_[c & 1], st));
+        };
+        issue(0);
+        for (size_t c = 0; c < nchunks; ++c) {
+            if (c + 1 < nchunks) issue(c + 1);
+            PTC_CUDA(cudaEventSynchronize(ev_[c & 1]));
+            const size_t off = c * kStage, n = std::min(kStage, bytes - off);
+            parallel_memcpy(static_cast<char*>(dst) + off, static_cast<const char*>(stage_[c & 1]), n);
+        }
+    }
+    ~HostCopier() {
+        for (int i = 0; i < 2; ++i) {
+            if (stage_[i]) cudaFreeHost(stage_[i]);
+            if (ev_[i]) cudaEventDestroy(ev_[i]);
+        }
+    }
+
+  private:
+    void ensure() {
+        if (stage_[0]) return;
+        for (int i = 0; i < 2; ++i) {
+            PTC_CUDA(cudaMallocHost(&stage_[i], kStage));
+            PTC_CUDA(cudaEventCreateWithFlags(&ev_[i], cudaEventDisableTiming));
+        }
+    }
+    static void parallel_memcpy(char* dst, const char* src, size_t n) {
+        constexpr size_t kBlock = 1ull << 20;
+        const int64_t nb = (int64_t)((n + kBlock - 1) / kBlock);
+#pragma omp parallel for schedule(static)
+        for (int64_t b = 0; b < nb; ++b) {
+            const size_t off = (size_t)b * kBlock;
+            std::memcpy(dst + off, src + off, std::min(kBlock, n - off));
+        }
+    }
+    void* stage_[2] = {nullptr, nullptr};
+    cudaEvent_t ev_[2] = {nullptr, nullptr};
+};
+
+// Host memory for a result: large blocks are 2 MiB aligned and marked for transparent huge
+// pages, so filling them costs far fewer page faults.  Released with free().
+void* host_result_alloc(size_t bytes) {
+    constexpr size_t kHuge = 2ull << 20;
+    if (bytes < (64ull << 20)) return std::malloc(bytes ? bytes : 1);
+    const size_t rounded = (bytes + kHuge - 1) / kHuge * kHuge;
+    void* p = std::aligned_alloc(kHuge, rounded);
+    if (p) madvise(p, rounded, MADV_HUGEPAGE);
+    return p;
+}
+
+HostCopier& host_copier() {
+    thread_local HostCopier c;
+    return c;
+}
+
 void print_reference_lines(const ptc_stats& s) {
     // the reference's stdout lines (fksCuckoo.hpp:1056-1057, fksCuckooTC.hpp:161,364-365)
     printf("Number of elements inserted = %llu\n", (unsigned long long)s.b_nnz);
@@ -196,8 +276,119 @@ void print_reference_lines(const ptc_stats& s) {
     fflush(stdout);
 }
 
+// the learned path sizes accumulators and the output for this many times the predicted count
+constexpr float kSizerMargin = 1.25f;
+
+const SizerHost* sizer_host(const ptc_sizer* s) { return s ? &s->host : nullptr; }
+
+// The sizer shipped beside the library (sizer_default.bin in the library's directory), if any.
+const SizerHost* default_sizer() {
+    static std::once_flag once;
+    static ptc_sizer* s = nullptr;
+    std::call_once(once, [] {
+        Dl_info info;
+        if (!dladdr(reinterpret_cast<void*>(&default_sizer), &info) || !info.dli_fname) return;
+        std::string path(info.dli_fname);
+        const size_t slash = path.rfind('/');
+        path = (slash == std::string::npos ? std::string(".") : path.substr(0, slash)) + "/sizer_default.bin";
+        ptc_sizer* loaded = nullptr;
+        if (ptc_sizer_load(path.c_str(), &loaded) == PTC_OK) s = loaded;
+    });
+    return s ? &s->host : nullptr;
+}
+
+// Grow the claimable output to `need` entries, keeping the first `used`.
+void grow_output(OutputView& ov, uint32_t od, uint64_t used, uint64_t need, cudaStream_t st) {
+    uint32_t* idx = nullptr;
+    double* val = nullptr;
+    PTC_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&idx), need * od * sizeof(uint32_t), st));
+    PTC_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&val), need * sizeof(double), st));
+    PTC_CUDA(cudaMemcpyAsync(idx, ov.idx, used * od * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+    PTC_CUDA(cudaMemcpyAsync(val, ov.val, used * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    PTC_CUDA(cudaFreeAsync(ov.idx, st));
+    PTC_CUDA(cudaFreeAsync(ov.val, st));
+    ov.idx = idx;
+    ov.val = val;
+    ov.capacity = need;
+}
+
+// Learned path, after the first numeric pass: parts whose accumulator or output claim did not
+// fit their prediction wrote nothing and are listed in ov.fail_list.  Their rows get the exact
+// symbolic pass, each failed part is re-split exactly, and the new parts run (their sizes are
+// exact, so they cannot fail again).  Returns the output nnz.
+uint64_t learned_reruns(const Operands& op, const PartItem* parts, uint32_t n_parts, const uint32_t* big_rows,
+                        uint32_t n_big, const float* pred, const SplitRule& rule, OutputView& ov,
+                        uint32_t* work_counter, uint32_t* err, int num_sms, uint64_t nrows, Arena& ar,
+                        ptc_stats& stats) {
+    cudaStream_t st = ar.stream();
+    const uint32_t P = op.npanels;
+    uint64_t* row_actual = ar.alloc<uint64_t>(nrows);
+    PTC_CUDA(cudaMemsetAsync(row_actual, 0, nrows * sizeof(uint64_t), st));
+    launch_row_actual(parts, ov.item_count, n_parts, row_actual, st);
+    const PartItem* cur = parts;
+    uint64_t rerun_rows = 0;
+    for (int round = 0;; ++round) {
+        const uint32_t nfail = read_scalar(ov.fail_count, st);
+        if (nfail == 0) break;
+        PTC_REQUIRE(round < 4, PTC_ERR_INTERNAL, "exactly sized parts failed again");
+        PartItem* failed = ar.alloc<PartItem>(nfail);
+        launch_gather_parts(cur, ov.fail_list, nfail, failed, st);
+        std::vector<PartItem> hf(nfail);
+        PTC_CUDA(cudaMemcpyAsync(hf.data(), failed, nfail * sizeof(PartItem), cudaMemcpyDeviceToHost, st));
+        PTC_CUDA(cudaStreamSynchronize(st));
+        std::vector<uint32_t> hrows, hridx(nfail);
+        std::vector<int64_t> seen;  // small: failed parts are few
+        for (uint32_t i = 0; i < nfail; ++i) {
+            uint32_t r = 0;
+            while (r < hrows.size() && hrows[r] != hf[i].row) ++r;
+            if (r == hrows.size()) hrows.push_back(hf[i].row);
+            hridx[i] = r;
+        }
+        const uint32_t nr = (uint32_t)hrows.size();
+        rerun_rows += nr;
+        uint32_t* drows = ar.alloc<uint32_t>(nr);
+        uint32_t* dridx = ar.alloc<uint32_t>(nfail);
+        PTC_CUDA(cudaMemcpyAsync(drows, hrows.data(), nr * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        PTC_CUDA(cudaMemcpyAsync(dridx, hridx.data(), nfail * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        uint32_t* cnt = ar.alloc<uint32_t>((uint64_t)nr * P);
+        uint64_t* scratch_d = ar.alloc<uint64_t>(nrows);
+        PTC_CUDA(cudaMemsetAsync(scratch_d, 0, nrows * sizeof(uint64_t), st));
+        launch_sym_bitmap(op, drows, nr, cnt, scratch_d, work_counter, num_sms, st);
+        uint32_t* np = ar.alloc<uint32_t>((uint64_t)nfail + 1);
+        uint32_t* tot = ar.alloc<uint32_t>(nfail);
+        launch_count_parts_range(failed, dridx, nfail, cnt, P, rule, np, tot, st);
+        exclusive_scan<uint32_t>(np, np, nfail, ar);
+        const uint32_t nnew = read_scalar(np + nfail, st);
+        uint64_t* need = ar.alloc<uint64_t>(1);
+        launch_sum_u32(tot, nfail, need, st);
+        const uint64_t used = read_scalar(ov.cursor, st);
+        const uint64_t want = used + read_scalar(need, st);
+        if (want > ov.capacity) grow_output(ov, op.fa + op.fb, used, want + 1024, st);
+        PartItem* fresh = ar.alloc<PartItem>(nnew);
+        launch_fill_parts_range(failed, dridx, nfail, cnt, P, rule, np, fresh, st);
+        ov.fail_list = ar.alloc<uint32_t>(std::max<uint32_t>(nnew, 1));
+        ov.item_count = ar.alloc<uint32_t>(std::max<uint32_t>(nnew, 1));
+        PTC_CUDA(cudaMemsetAsync(ov.fail_count, 0, sizeof(uint32_t), st));
+        launch_hash_parts(op, fresh, nnew, ov, work_counter, err, num_sms, st);
+        launch_row_actual(fresh, ov.item_count, nnew, row_actual, st);
+        cur = fresh;
+    }
+    stats.rerun_rows = rerun_rows;
+    double* esum = ar.alloc<double>(1);
+    launch_log2_error(big_rows, n_big, pred, row_actual, esum, st);
+    stats.sizer_mean_abs_log2_err = n_big ? read_scalar(esum, st) / n_big : 0.0;
+    return read_scalar(ov.cursor, st);
+}
+
+// Training samples of the learned sizer, gathered instead of running the numeric pass.
+struct Collect {
+    std::vector<float> x;  // n * kSizerInputs
+    std::vector<float> t;  // n
+};
+
 void contract_impl(const ptc_coo* A, const ptc_coo* Bin, uint32_t c, const uint32_t* a_modes,
-                   const uint32_t* b_modes_in, const ptc_options* opt_in, ptc_tensor* out, ptc_stats* stats_out) {
+                   const uint32_t* b_modes_in, const ptc_options* opt_in, ptc_tensor* out, ptc_stats* stats_out,
+                   Collect* collect = nullptr) {
     ptc_options opt;
     ptc_options_init(&opt);
     if (opt_in) {
@@ -228,9 +419,9 @@ void contract_impl(const ptc_coo* A, const ptc_coo* Bin, uint32_t c, const uint3
     if (self) PTC_REQUIRE(A->nnz > 1, PTC_ERR_TOO_FEW_NONZEROS, "Tensor B has at most one nonzeros");
     PTC_REQUIRE(opt.output_location == PTC_HOST || opt.output_location == PTC_DEVICE, PTC_ERR_INVALID_ARGUMENT,
                 "bad output_location");
-    PTC_REQUIRE(opt.panel_width == 0 || (opt.panel_width >= 256 && opt.panel_width <= 4096 &&
+    PTC_REQUIRE(opt.panel_width == 0 || (opt.panel_width >= 32 && opt.panel_width <= 4096 &&
                                          (opt.panel_width & (opt.panel_width - 1)) == 0),
-                PTC_ERR_INVALID_ARGUMENT, "panel_width must be 0 or a power of two in [256, 4096]");
+                PTC_ERR_INVALID_ARGUMENT, "panel_width must be 0 or a power of two in [32, 4096]");
 
     // device
     int ndev = 0;
@@ -358,7 +549,13 @@ void contract_impl(const ptc_coo* A, const ptc_coo* Bin, uint32_t c, const uint3
     // that each fit one shared-memory table (W <= table capacity, so a part always fits)
     PTC_REQUIRE(ncols <= sym_bitmap_max_cols(), PTC_ERR_INVALID_ARGUMENT,
                 "more than 1.5M distinct B free keys is not supported yet");
-    uint32_t W = opt.panel_width ? opt.panel_width : 4096;
+    // default: panels of 2048 columns (finer for narrow column spaces), the split table within 1 GiB
+    uint32_t W = opt.panel_width;
+    if (W == 0) {
+        W = 32;
+        while (W < 2048 && (uint64_t)W * 16 < ncols) W <<= 1;
+        while (W < 4096 && nfib * ((ncols + W - 1) / W + 1) * 4 > (1ull << 30)) W <<= 1;
+    }
     PTC_REQUIRE(W <= hash_part_capacity(), PTC_ERR_INVALID_ARGUMENT, "panel_width larger than a hash part");
     const uint32_t log2w = floor_log2(W);
     const uint32_t P = (uint32_t)std::max<uint64_t>(1, (ncols + W - 1) / W);
@@ -381,7 +578,27 @@ void contract_impl(const ptc_coo* A, const ptc_coo* Bin, uint32_t c, const uint3
     // row classes and work lists (largest rows first)
     uint32_t* small_flag = ar.alloc<uint32_t>(nrows + 1);
     uint32_t* big_flag = ar.alloc<uint32_t>(nrows + 1);
-    launch_classify_rows(row_flops, nrows, small_row_max_flops(), small_flag, big_flag, st);
+    uint32_t* esc_flag = ar.alloc<uint32_t>(nrows + 1);
+    launch_classify_rows(row_flops, rows.run_start, nrows, small_row_max_flops(), kEscMaxAvgProducts, small_flag,
+                         big_flag, esc_flag, st);
+    uint32_t* esc_pos = ar.alloc<uint32_t>(nrows + 1);
+    exclusive_scan<uint32_t>(esc_flag, esc_pos, nrows, ar);
+    uint32_t n_esc = read_scalar(esc_pos + nrows, st);
+    uint32_t* esc_rows = ar.alloc<uint32_t>(n_esc);
+    launch_compact_indices(esc_flag, esc_pos, nrows, esc_rows, st);
+    uint64_t* esc_off = ar.alloc<uint64_t>((uint64_t)n_esc + 1);
+    uint64_t f_esc = 0;
+    if (n_esc > 0) {
+        launch_esc_len(esc_rows, n_esc, row_flops, esc_off, st);
+        exclusive_scan<uint64_t>(esc_off, esc_off, n_esc, ar);
+        f_esc = read_scalar(esc_off + n_esc, st);
+        const int ebits = bits_for_space((uint64_t)n_esc), cbits2 = bits_for_space(std::max<uint64_t>(ncols, 1));
+        if (f_esc > kEscMaxProducts || ebits + cbits2 > 64) {  // too large for the sort buffers: hash path
+            launch_merge_flags(big_flag, esc_flag, nrows, st);
+            n_esc = 0;
+            f_esc = 0;
+        }
+    }
     uint32_t* small_pos = ar.alloc<uint32_t>(nrows + 1);
     uint32_t* big_pos = ar.alloc<uint32_t>(nrows + 1);
     exclusive_scan<uint32_t>(small_flag, small_pos, nrows, ar);
@@ -399,42 +616,139 @@ void contract_impl(const ptc_coo* A, const ptc_coo* Bin, uint32_t c, const uint3
     }
     stats.rows_small = n_small;
     stats.rows_hash = n_big;
+    stats.rows_long = n_esc;
 
-    // symbolic: exact output nnz per row (and per fine panel for the large rows)
+    const bool learned = opt.path == PTC_PATH_LEARNED && collect == nullptr;
+    const SizerHost* sizer = nullptr;
+    if (learned) {
+        sizer = opt.sizer ? sizer_host(opt.sizer) : default_sizer();
+        PTC_REQUIRE(sizer != nullptr, PTC_ERR_INVALID_ARGUMENT,
+                    "the learned path needs a sizer: opt.sizer, or sizer_default.bin beside the library");
+    }
+    SplitRule rule;
+    rule.cap = hash_part_capacity();
+    rule.dense_panels = dense_part_columns() >> log2w;
+    rule.dense_min = W / kDenseMinFraction;
+    rule.min_bits = hash_part_min_bits();
+
+    // symbolic: exact output nnz per row (and per fine panel for the large rows); the learned
+    // path counts only the sort-based rows (their sort gives the counts) and predicts the rest
     uint64_t* row_d = ar.alloc<uint64_t>(nrows + 1);
     PTC_CUDA(cudaMemsetAsync(row_d, 0, (nrows + 1) * sizeof(uint64_t), st));
     uint32_t* panel_cnt = ar.alloc<uint32_t>((uint64_t)n_big * P);
     uint32_t* work_counter = ar.alloc<uint32_t>(1);
     OutputView none;
-    launch_small_rows(false, op, small_rows, n_small, row_d, nullptr, none, st);
-    launch_sym_bitmap(op, big_rows, n_big, panel_cnt, row_d, work_counter, num_sms, st);
+    if (!learned) {
+        launch_small_rows(false, op, small_rows, n_small, row_d, nullptr, none, st);
+        launch_sym_bitmap(op, big_rows, n_big, panel_cnt, row_d, work_counter, num_sms, st);
+    }
+    // sort-based rows: expand their products in stream order, sort stably by (row, column)
+    const uint32_t esc_colbits = (uint32_t)colbits;
+    uint64_t* esc_key = nullptr;
+    double* esc_val = nullptr;
+    uint32_t* esc_perm = nullptr;
+    uint32_t* esc_run_start = nullptr;
+    uint64_t* esc_run_key = nullptr;
+    uint32_t* esc_first = nullptr;
+    uint64_t esc_runs = 0;
+    if (n_esc > 0) {
+        int32_t* esc_of = ar.alloc<int32_t>(nrows);
+        PTC_CUDA(cudaMemsetAsync(esc_of, 0xff, nrows * sizeof(int32_t), st));
+        launch_esc_index(esc_rows, n_esc, esc_of, st);
+        esc_key = ar.alloc<uint64_t>(f_esc);
+        esc_val = ar.alloc<double>(f_esc);
+        esc_perm = ar.alloc<uint32_t>(f_esc);
+        launch_esc_expand(op, rows.run_of, esc_of, alen, esc_off, esc_colbits, esc_key, esc_val, esc_perm, st);
+        radix_sort_pairs(esc_key, esc_perm, f_esc, 0, esc_colbits + bits_for_space((uint64_t)n_esc), ar);
+        esc_run_start = ar.alloc<uint32_t>(f_esc + 1);
+        esc_run_key = ar.alloc<uint64_t>(f_esc);
+        esc_runs = runs_of_sorted(esc_key, f_esc, nullptr, esc_run_start, esc_run_key, ar);
+        esc_first = ar.alloc<uint32_t>(n_esc);
+        launch_esc_count(esc_run_key, esc_runs, esc_colbits, esc_rows, row_d, esc_first, st);
+    }
     uint64_t* row_off = ar.alloc<uint64_t>(nrows + 1);
     exclusive_scan<uint64_t>(row_d, row_off, nrows, ar);
-    const uint64_t out_nnz = read_scalar(row_off + nrows, st);
+    const uint64_t exact_nnz = read_scalar(row_off + nrows, st);  // all rows, or sort-based rows only
+    if (collect) {
+        // features of the rows the learned path sizes, and log2(1 + their exact output nnz)
+        float* gp = ar.alloc<float>((uint64_t)(P + 1) * kGridPoints);
+        launch_popularity_table(b_col, nb, ncols, P, log2w, gp, ar);
+        float* fx = ar.alloc<float>((uint64_t)n_big * kSizerInputs);
+        float* ft = ar.alloc<float>(n_big);
+        launch_row_features(op, big_rows, n_big, row_flops, gp, fx, st);
+        launch_row_targets(big_rows, n_big, row_d, ft, st);
+        collect->x.resize((uint64_t)n_big * kSizerInputs);
+        collect->t.resize(n_big);
+        PTC_CUDA(cudaMemcpyAsync(collect->x.data(), fx, collect->x.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+        PTC_CUDA(cudaMemcpyAsync(collect->t.data(), ft, collect->t.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+        ar.release();
+        PTC_CUDA(cudaStreamSynchronize(st));
+        stats.out_nnz = exact_nnz;
+        if (stats_out) *stats_out = stats;
+        return;
+    }
+
+    float* pred = nullptr;
+    uint64_t capacity = exact_nnz;
+    if (learned && n_big > 0) {
+        // sizer: per-row features -> predicted log2(1 + nnz) -> per-panel counts by column popularity
+        float* gp = ar.alloc<float>((uint64_t)(P + 1) * kGridPoints);
+        launch_popularity_table(b_col, nb, ncols, P, log2w, gp, ar);
+        float* fx = ar.alloc<float>((uint64_t)n_big * kSizerInputs);
+        launch_row_features(op, big_rows, n_big, row_flops, gp, fx, st);
+        pred = ar.alloc<float>(n_big);
+        sizer_predict_device(*sizer, fx, n_big, pred, ar);
+        launch_predicted_panel_counts(big_rows, n_big, row_flops, pred, gp, P, log2w, ncols, kSizerMargin, panel_cnt,
+                                      st);
+        uint64_t* psum = ar.alloc<uint64_t>(1);
+        launch_sum_u32(panel_cnt, (uint64_t)n_big * P, psum, st);
+        capacity += read_scalar(psum, st);
+    }
+    if (learned) capacity += (uint64_t)n_small * small_row_max_flops() + 1024;
 
     // split large rows into parts that fit a shared-memory table
     uint32_t* nparts = ar.alloc<uint32_t>((uint64_t)n_big + 1);
-    launch_count_parts(panel_cnt, n_big, P, hash_part_capacity(), nparts, err, st);
+    launch_count_parts(panel_cnt, n_big, P, rule, nparts, err, st);
     exclusive_scan<uint32_t>(nparts, nparts, n_big, ar);
     const uint32_t n_parts = read_scalar(nparts + n_big, st);
     PTC_REQUIRE(read_scalar(err, st) == 0, PTC_ERR_INTERNAL, "a fine panel exceeds the hash part capacity");
     PartItem* parts = ar.alloc<PartItem>(n_parts);
-    launch_fill_parts(big_rows, panel_cnt, n_big, P, hash_part_capacity(), nparts, row_off, parts, st);
+    launch_fill_parts(big_rows, panel_cnt, n_big, P, rule, nparts, learned ? nullptr : row_off, parts, st);
     stats.hash_parts = n_parts;
     PTC_CUDA(cudaEventRecord(ev.ev[EV_SYM], st));
 
     // ---- numeric ----
     const uint32_t od = fa + fb;
     OutputView ov;
-    PTC_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&ov.idx), std::max<uint64_t>(out_nnz * od, 1) * sizeof(uint32_t), st));
-    PTC_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&ov.val), std::max<uint64_t>(out_nnz, 1) * sizeof(double), st));
-    launch_small_rows(true, op, small_rows, n_small, nullptr, row_off, ov, st);
-    launch_hash_parts(op, parts, n_parts, ov, work_counter, err, num_sms, st);
-    PTC_CUDA(cudaEventRecord(ev.ev[EV_NUM], st));
-    if (read_scalar(err, st) != 0) {
+    PTC_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&ov.idx), std::max<uint64_t>(capacity * od, 1) * sizeof(uint32_t), st));
+    PTC_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&ov.val), std::max<uint64_t>(capacity, 1) * sizeof(double), st));
+    uint64_t out_nnz = exact_nnz;
+    try {
+        if (learned) {
+            ov.capacity = capacity;
+            ov.cursor = ar.alloc<uint64_t>(1);
+            ov.fail_count = ar.alloc<uint32_t>(1);
+            ov.fail_list = ar.alloc<uint32_t>(std::max<uint32_t>(n_parts, 1));
+            ov.item_count = ar.alloc<uint32_t>(std::max<uint32_t>(n_parts, 1));
+            PTC_CUDA(cudaMemcpyAsync(ov.cursor, &exact_nnz, sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+            PTC_CUDA(cudaMemsetAsync(ov.fail_count, 0, sizeof(uint32_t), st));
+        }
+        launch_small_rows(true, op, small_rows, n_small, nullptr, learned ? nullptr : row_off, ov, st);
+        launch_hash_parts(op, parts, n_parts, ov, work_counter, err, num_sms, st);
+        if (n_esc > 0)
+            launch_esc_fold(op, ov, esc_run_key, esc_run_start, esc_runs, esc_colbits, esc_rows, esc_first, row_off,
+                            esc_perm, esc_val, f_esc, reinterpret_cast<double*>(esc_key), st);
+        if (learned) {
+            out_nnz = learned_reruns(op, parts, n_parts, big_rows, n_big, pred, rule, ov, work_counter, err, num_sms,
+                                     nrows, ar, stats);
+        }
+        PTC_CUDA(cudaEventRecord(ev.ev[EV_NUM], st));
+        PTC_REQUIRE(read_scalar(err, st) == 0, PTC_ERR_INTERNAL,
+                    "an accumulator table overflowed or met an out-of-range column");
+    } catch (...) {
         cudaFreeAsync(ov.idx, st);
         cudaFreeAsync(ov.val, st);
-        throw Error{PTC_ERR_INTERNAL, "an accumulator table overflowed or met an out-of-range column"};
+        throw;
     }
 
     // ---- output ----
@@ -447,8 +761,8 @@ void contract_impl(const ptc_coo* A, const ptc_coo* Bin, uint32_t c, const uint3
         PTC_CUDA(cudaEventRecord(ev.ev[EV_D2H], st));
     } else {
         out->location = PTC_HOST;
-        out->idx = static_cast<uint32_t*>(std::malloc(std::max<uint64_t>(out_nnz * od, 1) * sizeof(uint32_t)));
-        out->vals = static_cast<double*>(std::malloc(std::max<uint64_t>(out_nnz, 1) * sizeof(double)));
+        out->idx = static_cast<uint32_t*>(host_result_alloc(out_nnz * od * sizeof(uint32_t)));
+        out->vals = static_cast<double*>(host_result_alloc(out_nnz * sizeof(double)));
         if (!out->idx || !out->vals) {
             std::free(out->idx);
             std::free(out->vals);
@@ -458,8 +772,8 @@ void contract_impl(const ptc_coo* A, const ptc_coo* Bin, uint32_t c, const uint3
             out->vals = nullptr;
             throw Error{PTC_ERR_OUT_OF_MEMORY, "host output allocation failed"};
         }
-        PTC_CUDA(cudaMemcpyAsync(out->idx, ov.idx, out_nnz * od * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-        PTC_CUDA(cudaMemcpyAsync(out->vals, ov.val, out_nnz * sizeof(double), cudaMemcpyDeviceToHost, st));
+        host_copier().copy(out->idx, ov.idx, out_nnz * od * sizeof(uint32_t), st);
+        host_copier().copy(out->vals, ov.val, out_nnz * sizeof(double), st);
         PTC_CUDA(cudaFreeAsync(ov.idx, st));
         PTC_CUDA(cudaFreeAsync(ov.val, st));
         PTC_CUDA(cudaEventRecord(ev.ev[EV_D2H], st));
@@ -533,6 +847,31 @@ ptc_status ptc_contract(const ptc_coo* A, const ptc_coo* B, uint32_t c, const ui
     } catch (const std::bad_alloc&) {
         ptc::set_last_error(PTC_ERR_OUT_OF_MEMORY, "host allocation failed");
         return PTC_ERR_OUT_OF_MEMORY;
+    } catch (...) {
+        ptc::set_last_error(PTC_ERR_INTERNAL, "unexpected exception");
+        return PTC_ERR_INTERNAL;
+    }
+}
+
+ptc_status ptc_sizer_collect(const ptc_coo* A, const ptc_coo* B, uint32_t c, const uint32_t* a_modes,
+                             const uint32_t* b_modes, const ptc_options* opt, float** features, float** targets,
+                             uint64_t* n) {
+    try {
+        PTC_REQUIRE(features && targets && n, PTC_ERR_INVALID_ARGUMENT, "null output argument");
+        ptc::Collect col;
+        ptc_tensor dummy;
+        ptc::contract_impl(A, B, c, a_modes, b_modes, opt, &dummy, nullptr, &col);
+        *n = col.t.size();
+        *features = static_cast<float*>(std::malloc(std::max<size_t>(col.x.size(), 1) * sizeof(float)));
+        *targets = static_cast<float*>(std::malloc(std::max<size_t>(col.t.size(), 1) * sizeof(float)));
+        PTC_REQUIRE(*features && *targets, PTC_ERR_OUT_OF_MEMORY, "host allocation failed");
+        std::memcpy(*features, col.x.data(), col.x.size() * sizeof(float));
+        std::memcpy(*targets, col.t.data(), col.t.size() * sizeof(float));
+        ptc::g_last_error.clear();
+        return PTC_OK;
+    } catch (const Error& e) {
+        ptc::set_last_error(e.status, e.msg);
+        return e.status;
     } catch (...) {
         ptc::set_last_error(PTC_ERR_INTERNAL, "unexpected exception");
         return PTC_ERR_INTERNAL;

@@ -55,15 +55,40 @@ struct PartItem {
     uint32_t row;
     uint32_t p0;
     uint32_t p1;
-    uint32_t pad;
+    uint32_t mode;  // bit 0: 1 = dense (direct-mapped by column), 0 = open-addressing table of
+                    // 2^(mode >> 1) slots
     uint64_t out_off;
 };
 
 // Output destination.
+// Output destination.  Work items with exact offsets write there directly.  Items whose offset is
+// kClaimOffset (the learned path, where exact counts are not known in advance) claim a range
+// from *cursor once their count is known; a claim that would pass `capacity`, or an item whose
+// accumulator overflowed, writes nothing and is appended to fail_list for an exact rerun.
+constexpr uint64_t kClaimOffset = ~0ull;
+
 struct OutputView {
-    uint32_t* idx = nullptr;   // [nnz * (fa + fb)]
-    double* val = nullptr;     // [nnz]
+    uint32_t* idx = nullptr;        // [capacity * (fa + fb)]
+    double* val = nullptr;          // [capacity]
+    uint64_t* cursor = nullptr;     // next free entry (claim mode)
+    uint64_t capacity = 0;          // entries available (claim mode)
+    uint32_t* fail_list = nullptr;  // items to rerun exactly
+    uint32_t* fail_count = nullptr;
+    uint32_t* item_count = nullptr; // optional: entries written by each item
 };
+
+// Claim `n` entries at the output cursor without passing the capacity; ~0 if they do not fit.
+__device__ __forceinline__ uint64_t claim_output(const OutputView& out, uint64_t n) {
+    unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(out.cursor);
+    for (int tries = 0; tries < (1 << 20); ++tries) {
+        if (cur + n > out.capacity) return ~0ull;
+        const unsigned long long prev =
+            atomicCAS(reinterpret_cast<unsigned long long*>(out.cursor), cur, cur + n);
+        if (prev == cur) return cur;
+        cur = prev;
+    }
+    return ~0ull;
+}
 
 void launch_pack_keys(const uint32_t* idx, uint64_t nnz, const DimSpec& dims, const KeySpec& k1,
                       const KeySpec& k2, uint64_t* key1, uint64_t* key2, uint32_t* err, cudaStream_t st);

@@ -1,0 +1,116 @@
+// Learned-path planning: predicted per-panel counts from the sizer, and the bookkeeping of the
+// exact reruns of parts whose prediction was too small.
+#include <cmath>
+
+#include "ptc_learned.cuh"
+
+namespace ptc {
+
+// G_p(F) of the popularity table (see ptc_sizer.cuh), linear in log2 F between grid points
+__device__ __forceinline__ float popularity_at(const float* __restrict__ row, float F) {
+    if (F <= 1.f) return F * row[0];
+    float u = fminf(log2f(F) * kGridPerOctave, (float)(kGridPoints - 1));
+    const int g = (int)u;
+    const float fr = u - (float)g;
+    const float a = row[g], b = row[min(g + 1, kGridPoints - 1)];
+    return a + fr * (b - a);
+}
+
+// cnt[i * P + p] = ceil(margin * D_pred(i) * G_p(F_i) / G(F_i)), at most the panel's width and
+// the row's products; D_pred = 2^pred - 1 clamped to [1, min(F, ncols)].
+__global__ void predicted_panel_counts_kernel(const uint32_t* __restrict__ rows, uint64_t n,
+                                              const uint64_t* __restrict__ row_flops, const float* __restrict__ pred,
+                                              const float* __restrict__ gp, uint32_t P, uint32_t panel_log2,
+                                              uint64_t ncols, float margin, uint32_t* __restrict__ cnt) {
+    const uint64_t id = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= n * P) return;
+    const uint64_t i = id / P;
+    const uint32_t p = (uint32_t)(id % P);
+    const float F = (float)row_flops[rows[i]];
+    float d = exp2f(pred[i]) - 1.f;
+    d = fminf(fmaxf(d, 1.f), fminf(F, (float)ncols));
+    const float tot = popularity_at(gp + (uint64_t)P * kGridPoints, F);
+    const float share = tot > 0.f ? popularity_at(gp + (uint64_t)p * kGridPoints, F) / tot : 1.f / P;
+    const uint64_t lo = (uint64_t)p << panel_log2;
+    const uint64_t width = (ncols - lo) < (1ull << panel_log2) ? (ncols - lo) : (1ull << panel_log2);
+    float c = ceilf(margin * d * share);
+    c = fminf(fminf(c, (float)width), F);
+    cnt[id] = (uint32_t)c;
+}
+
+void launch_predicted_panel_counts(const uint32_t* rows, uint64_t n, const uint64_t* row_flops, const float* pred,
+                                   const float* gp, uint32_t P, uint32_t panel_log2, uint64_t ncols, float margin,
+                                   uint32_t* cnt, cudaStream_t st) {
+    if (n == 0) return;
+    predicted_panel_counts_kernel<<<ceil_div_u32(n * P, 256), 256, 0, st>>>(rows, n, row_flops, pred, gp, P,
+                                                                           panel_log2, ncols, margin, cnt);
+    count_launch();
+    PTC_CHECK_LAUNCH();
+}
+
+__global__ void sum_u32_kernel(const uint32_t* __restrict__ x, uint64_t n, unsigned long long* __restrict__ out) {
+    uint64_t acc = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        acc += x[i];
+    acc = warp_sum(acc);
+    if (lane_id() == 0 && acc) atomicAdd(out, (unsigned long long)acc);
+}
+
+void launch_sum_u32(const uint32_t* x, uint64_t n, uint64_t* out, cudaStream_t st) {
+    PTC_CUDA(cudaMemsetAsync(out, 0, sizeof(uint64_t), st));
+    if (n == 0) return;
+    const uint32_t grid = std::min<uint32_t>(ceil_div_u32(n, 256), 1024);
+    sum_u32_kernel<<<grid, 256, 0, st>>>(x, n, reinterpret_cast<unsigned long long*>(out));
+    count_launch();
+    PTC_CHECK_LAUNCH();
+}
+
+__global__ void gather_parts_kernel(const PartItem* __restrict__ parts, const uint32_t* __restrict__ idx, uint32_t n,
+                                    PartItem* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = parts[idx[i]];
+}
+
+void launch_gather_parts(const PartItem* parts, const uint32_t* idx, uint32_t n, PartItem* out, cudaStream_t st) {
+    if (n == 0) return;
+    gather_parts_kernel<<<ceil_div_u32(n, 256), 256, 0, st>>>(parts, idx, n, out);
+    count_launch();
+    PTC_CHECK_LAUNCH();
+}
+
+__global__ void row_actual_kernel(const PartItem* __restrict__ parts, const uint32_t* __restrict__ counts, uint32_t n,
+                                  uint64_t* __restrict__ row_actual) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && counts[i])
+        atomicAdd(reinterpret_cast<unsigned long long*>(&row_actual[parts[i].row]), (unsigned long long)counts[i]);
+}
+
+void launch_row_actual(const PartItem* parts, const uint32_t* counts, uint32_t n, uint64_t* row_actual,
+                       cudaStream_t st) {
+    if (n == 0) return;
+    row_actual_kernel<<<ceil_div_u32(n, 256), 256, 0, st>>>(parts, counts, n, row_actual);
+    count_launch();
+    PTC_CHECK_LAUNCH();
+}
+
+// sum over rows of |pred_i - log2(1 + actual(row_i))|
+__global__ void log2_error_kernel(const uint32_t* __restrict__ rows, uint64_t n, const float* __restrict__ pred,
+                                  const uint64_t* __restrict__ row_actual, double* __restrict__ out) {
+    double acc = 0.0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        acc += fabs((double)pred[i] - log2(1.0 + (double)row_actual[rows[i]]));
+    acc = warp_sum(acc);
+    if (lane_id() == 0) atomicAdd(out, acc);
+}
+
+void launch_log2_error(const uint32_t* rows, uint64_t n, const float* pred, const uint64_t* row_actual, double* out,
+                       cudaStream_t st) {
+    PTC_CUDA(cudaMemsetAsync(out, 0, sizeof(double), st));
+    if (n == 0) return;
+    const uint32_t grid = std::min<uint32_t>(ceil_div_u32(n, 256), 1024);
+    log2_error_kernel<<<grid, 256, 0, st>>>(rows, n, pred, row_actual, out);
+    count_launch();
+    PTC_CHECK_LAUNCH();
+}
+
+}  // namespace ptc

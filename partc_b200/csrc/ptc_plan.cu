@@ -1,21 +1,42 @@
 // Planning kernels: row classes, work lists, and the split of large rows into hash parts.
+#include "ptc_learned.cuh"
 #include "ptc_spa.cuh"
 
 namespace ptc {
 
-__global__ void classify_rows_kernel(const uint64_t* __restrict__ row_flops, uint64_t nrows, uint64_t small_max,
-                                     uint32_t* __restrict__ small_flag, uint32_t* __restrict__ big_flag) {
+__global__ void classify_rows_kernel(const uint64_t* __restrict__ row_flops, const uint32_t* __restrict__ row_start,
+                                     uint64_t nrows, uint64_t small_max, uint32_t esc_avg,
+                                     uint32_t* __restrict__ small_flag, uint32_t* __restrict__ big_flag,
+                                     uint32_t* __restrict__ esc_flag) {
     const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= nrows) return;
-    const uint64_t f = row_flops[r];
-    small_flag[r] = (f > 0 && f <= small_max) ? 1u : 0u;  // rows without products are skipped
-    big_flag[r] = (f > small_max) ? 1u : 0u;              // (fksCuckooTC.hpp:183)
+    const uint64_t f = row_flops[r];  // rows without products are skipped (fksCuckooTC.hpp:183)
+    const uint64_t len = row_start[r + 1] - row_start[r];
+    const bool small = f > 0 && f <= small_max;
+    const bool esc = f > small_max && f < (uint64_t)esc_avg * len;
+    small_flag[r] = small ? 1u : 0u;
+    esc_flag[r] = esc ? 1u : 0u;
+    big_flag[r] = (f > small_max && !esc) ? 1u : 0u;
 }
 
-void launch_classify_rows(const uint64_t* row_flops, uint64_t nrows, uint64_t small_max, uint32_t* small_flag,
-                          uint32_t* big_flag, cudaStream_t st) {
+void launch_classify_rows(const uint64_t* row_flops, const uint32_t* row_start, uint64_t nrows, uint64_t small_max,
+                          uint32_t esc_avg, uint32_t* small_flag, uint32_t* big_flag, uint32_t* esc_flag,
+                          cudaStream_t st) {
     if (nrows == 0) return;
-    classify_rows_kernel<<<ceil_div_u32(nrows, 256), 256, 0, st>>>(row_flops, nrows, small_max, small_flag, big_flag);
+    classify_rows_kernel<<<ceil_div_u32(nrows, 256), 256, 0, st>>>(row_flops, row_start, nrows, small_max, esc_avg,
+                                                                   small_flag, big_flag, esc_flag);
+    count_launch();
+    PTC_CHECK_LAUNCH();
+}
+
+__global__ void merge_flags_kernel(uint32_t* __restrict__ big_flag, const uint32_t* __restrict__ esc_flag, uint64_t n) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) big_flag[i] |= esc_flag[i];
+}
+
+void launch_merge_flags(uint32_t* big_flag, const uint32_t* esc_flag, uint64_t nrows, cudaStream_t st) {
+    if (nrows == 0) return;
+    merge_flags_kernel<<<ceil_div_u32(nrows, 256), 256, 0, st>>>(big_flag, esc_flag, nrows);
     count_launch();
     PTC_CHECK_LAUNCH();
 }
@@ -46,71 +67,149 @@ void launch_work_keys(const uint32_t* rows, uint64_t n, const uint64_t* row_flop
     PTC_CHECK_LAUNCH();
 }
 
-// Greedy split of one row's fine panels into consecutive groups holding at most `cap` entries.
-// Calls emit(p0, p1, entries_before_p0) for each group; returns the number of groups.
+// Split one row's fine panels into parts (see SplitRule).  Calls emit(p0, p1, entries_before,
+// mode) for each non-empty part; returns the number of parts.  The dense-window sums slide
+// forward with p, so a row costs O(P).
 template <typename Emit>
-__device__ __forceinline__ uint32_t split_panels(const uint32_t* cnt, uint32_t P, uint32_t cap, bool* oversize,
+__device__ __forceinline__ uint32_t split_panels(const uint32_t* cnt, uint32_t P, SplitRule rule, bool* oversize,
                                                  Emit emit) {
-    uint32_t groups = 0, p0 = 0, acc = 0;
+    uint32_t parts = 0, p = 0;
     uint64_t before = 0;
-    for (uint32_t p = 0; p < P; ++p) {
-        const uint32_t c = cnt[p];
-        if (c > cap) *oversize = true;
-        if (acc > 0 && acc + c > cap) {
-            emit(p0, p, before);
-            ++groups;
-            before += acc;
-            p0 = p;
-            acc = 0;
+    uint64_t wsum = 0;
+    uint32_t wlo = 0, whi = 0;  // window [wlo, whi) with running sum wsum
+    auto dense_window = [&](uint32_t q, uint32_t& w, uint64_t& sum) {
+        if (rule.dense_panels == 0) return false;
+        const uint32_t hi = min(q + rule.dense_panels, P);
+        while (whi < hi) wsum += cnt[whi++];
+        while (wlo < q) wsum -= cnt[wlo++];
+        w = hi - q;
+        sum = wsum;
+        return sum >= (uint64_t)rule.dense_min * w;
+    };
+    while (p < P) {
+        uint32_t w;
+        uint64_t sum;
+        if (dense_window(p, w, sum)) {
+            emit(p, p + w, before, 1u);
+            ++parts;
+            before += sum;
+            p += w;
+            continue;
         }
-        acc += c;
+        const uint32_t p0 = p;
+        uint64_t acc = 0;
+        while (p < P && (acc == 0 || acc + cnt[p] <= rule.cap)) {
+            if (cnt[p] > rule.cap) *oversize = true;
+            acc += cnt[p];
+            ++p;
+            uint32_t w2;
+            uint64_t s2;
+            if (p < P && dense_window(p, w2, s2)) break;
+        }
+        if (acc > 0) {
+            // table of at least acc / 0.75 slots, a power of two
+            uint32_t bits = rule.min_bits;
+            while (bits < 13 && ((uint64_t)3 << bits) < acc * 4) ++bits;
+            emit(p0, p, before, bits << 1);
+            ++parts;
+            before += acc;
+        }
     }
-    emit(p0, P, before);
-    return groups + 1;
+    return parts;
 }
 
-__global__ void count_parts_kernel(const uint32_t* __restrict__ panel_cnt, uint64_t nbig, uint32_t P, uint32_t cap,
+__global__ void count_parts_kernel(const uint32_t* __restrict__ panel_cnt, uint64_t nbig, uint32_t P, SplitRule rule,
                                    uint32_t* __restrict__ nparts, uint32_t* __restrict__ oversize) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nbig) return;
     bool over = false;
-    nparts[i] = split_panels(panel_cnt + i * P, P, cap, &over, [](uint32_t, uint32_t, uint64_t) {});
+    nparts[i] = split_panels(panel_cnt + i * P, P, rule, &over, [](uint32_t, uint32_t, uint64_t, uint32_t) {});
     if (over) atomicOr(oversize, 1u);
 }
 
-void launch_count_parts(const uint32_t* panel_cnt, uint64_t nbig, uint32_t npanels, uint32_t cap, uint32_t* nparts,
+void launch_count_parts(const uint32_t* panel_cnt, uint64_t nbig, uint32_t npanels, SplitRule rule, uint32_t* nparts,
                         uint32_t* oversize, cudaStream_t st) {
     if (nbig == 0) return;
-    count_parts_kernel<<<ceil_div_u32(nbig, 256), 256, 0, st>>>(panel_cnt, nbig, npanels, cap, nparts, oversize);
+    count_parts_kernel<<<ceil_div_u32(nbig, 256), 256, 0, st>>>(panel_cnt, nbig, npanels, rule, nparts, oversize);
     count_launch();
     PTC_CHECK_LAUNCH();
 }
 
 __global__ void fill_parts_kernel(const uint32_t* __restrict__ rows, const uint32_t* __restrict__ panel_cnt,
-                                  uint64_t nbig, uint32_t P, uint32_t cap, const uint32_t* __restrict__ part_pos,
+                                  uint64_t nbig, uint32_t P, SplitRule rule, const uint32_t* __restrict__ part_pos,
                                   const uint64_t* __restrict__ row_off, PartItem* __restrict__ parts) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nbig) return;
     const uint32_t row = rows[i];
-    const uint64_t base = row_off[row];
+    const uint64_t base = row_off ? row_off[row] : 0;  // no offsets: the parts claim output later
     uint32_t o = part_pos[i];
     bool over = false;
-    split_panels(panel_cnt + i * P, P, cap, &over, [&](uint32_t p0, uint32_t p1, uint64_t before) {
+    split_panels(panel_cnt + i * P, P, rule, &over, [&](uint32_t p0, uint32_t p1, uint64_t before, uint32_t mode) {
         PartItem it;
         it.row = row;
         it.p0 = p0;
         it.p1 = p1;
-        it.pad = 0;
-        it.out_off = base + before;
+        it.mode = mode;
+        it.out_off = row_off ? base + before : kClaimOffset;
         parts[o++] = it;
     });
 }
 
-void launch_fill_parts(const uint32_t* rows, const uint32_t* panel_cnt, uint64_t nbig, uint32_t npanels, uint32_t cap,
+void launch_fill_parts(const uint32_t* rows, const uint32_t* panel_cnt, uint64_t nbig, uint32_t npanels, SplitRule rule,
                        const uint32_t* part_pos, const uint64_t* row_off, PartItem* parts, cudaStream_t st) {
     if (nbig == 0) return;
-    fill_parts_kernel<<<ceil_div_u32(nbig, 256), 256, 0, st>>>(rows, panel_cnt, nbig, npanels, cap, part_pos, row_off,
+    fill_parts_kernel<<<ceil_div_u32(nbig, 256), 256, 0, st>>>(rows, panel_cnt, nbig, npanels, rule, part_pos, row_off,
                                                                parts);
+    count_launch();
+    PTC_CHECK_LAUNCH();
+}
+
+__global__ void count_parts_range_kernel(const PartItem* __restrict__ parts, const uint32_t* __restrict__ ridx,
+                                         uint32_t n, const uint32_t* __restrict__ panel_cnt, uint32_t P, SplitRule rule,
+                                         uint32_t* __restrict__ nparts, uint32_t* __restrict__ total) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const PartItem it = parts[i];
+    const uint32_t* cnt = panel_cnt + (uint64_t)ridx[i] * P;
+    uint64_t tot = 0;
+    for (uint32_t p = it.p0; p < it.p1; ++p) tot += cnt[p];
+    total[i] = (uint32_t)tot;
+    bool over = false;
+    nparts[i] = split_panels(cnt + it.p0, it.p1 - it.p0, rule, &over, [](uint32_t, uint32_t, uint64_t, uint32_t) {});
+}
+
+void launch_count_parts_range(const PartItem* parts, const uint32_t* ridx, uint32_t n, const uint32_t* panel_cnt,
+                              uint32_t P, SplitRule rule, uint32_t* nparts, uint32_t* total, cudaStream_t st) {
+    if (n == 0) return;
+    count_parts_range_kernel<<<ceil_div_u32(n, 128), 128, 0, st>>>(parts, ridx, n, panel_cnt, P, rule, nparts, total);
+    count_launch();
+    PTC_CHECK_LAUNCH();
+}
+
+__global__ void fill_parts_range_kernel(const PartItem* __restrict__ parts, const uint32_t* __restrict__ ridx,
+                                        uint32_t n, const uint32_t* __restrict__ panel_cnt, uint32_t P, SplitRule rule,
+                                        const uint32_t* __restrict__ part_pos, PartItem* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const PartItem it = parts[i];
+    const uint32_t* cnt = panel_cnt + (uint64_t)ridx[i] * P;
+    uint32_t o = part_pos[i];
+    bool over = false;
+    split_panels(cnt + it.p0, it.p1 - it.p0, rule, &over, [&](uint32_t q0, uint32_t q1, uint64_t, uint32_t mode) {
+        PartItem x;
+        x.row = it.row;
+        x.p0 = it.p0 + q0;
+        x.p1 = it.p0 + q1;
+        x.mode = mode;
+        x.out_off = kClaimOffset;
+        out[o++] = x;
+    });
+}
+
+void launch_fill_parts_range(const PartItem* parts, const uint32_t* ridx, uint32_t n, const uint32_t* panel_cnt,
+                             uint32_t P, SplitRule rule, const uint32_t* part_pos, PartItem* out, cudaStream_t st) {
+    if (n == 0) return;
+    fill_parts_range_kernel<<<ceil_div_u32(n, 128), 128, 0, st>>>(parts, ridx, n, panel_cnt, P, rule, part_pos, out);
     count_launch();
     PTC_CHECK_LAUNCH();
 }

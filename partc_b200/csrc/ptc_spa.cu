@@ -163,13 +163,28 @@ __global__ void __launch_bounds__(kSmallWarps * 32)
             }
         }
         // emit (numeric) or count (symbolic), resetting the table
-        uint64_t o = NUMERIC ? row_off[row] : 0;
+        uint64_t o = 0;
+        if (NUMERIC) {
+            if (row_off) {
+                o = row_off[row];
+            } else {  // claim mode: count first, then take a range at the output cursor
+                uint32_t cnt = 0;
+                for (uint32_t i = 0; i < kSmallSlots; i += 32)
+                    cnt += __popc(__ballot_sync(kFullMask, keys[i + lane] != kEmptyCol));
+                if (lane == 0) {
+                    o = claim_output(out, cnt);
+                    if (o == ~0ull) atomicOr(op.err, 2u);  // capacity is reserved for these rows
+                }
+                o = __shfl_sync(kFullMask, o, 0);
+            }
+        }
+        const bool write = NUMERIC && o != ~0ull;
         for (uint32_t i = 0; i < kSmallSlots; i += 32) {
             const uint32_t sidx = i + lane;
             const uint32_t kc = keys[sidx];
             const bool occ = kc != kEmptyCol;
             const uint32_t mask = __ballot_sync(kFullMask, occ);
-            if (NUMERIC && occ) write_entry(op, out, o + __popc(mask & lanemask_lt()), row, kc, vals[sidx]);
+            if (write && occ) write_entry(op, out, o + __popc(mask & lanemask_lt()), row, kc, vals[sidx]);
             keys[sidx] = kEmptyCol;
             o += __popc(mask);
         }
@@ -200,6 +215,7 @@ void launch_small_rows(bool numeric, const Operands& op, const uint32_t* rows, u
 // ---------------------------------------------------------------------------------------------
 
 constexpr int kSymThreads = 512;
+constexpr int kSymItems = 4;
 
 __global__ void __launch_bounds__(kSymThreads)
     sym_bitmap_kernel(Operands op, const uint32_t* __restrict__ rows, uint32_t nrows, uint32_t* __restrict__ panel_cnt,
@@ -239,17 +255,31 @@ __global__ void __launch_bounds__(kSymThreads)
             wl[t] = L;
             wscan[t] = excl;
             __syncthreads();
-            uint32_t kk = 0;
-            for (uint32_t p = t; p < total; p += kSymThreads) {
-                while (kk + 1 < kSymThreads && wscan[kk] + wl[kk] <= p) ++kk;
-                const uint32_t col = op.b_col[ws[kk] + (p - wscan[kk])];
-                const uint32_t bit = 1u << (col & 31);
-                const uint32_t old = atomicOr(&bits[col >> 5], bit);
-                const bool fresh = !(old & bit);
-                const uint32_t active = __activemask();
-                const uint32_t panel = fresh ? (col >> op.panel_log2) : 0xffffffffu;
-                const uint32_t m = __match_any_sync(active, panel);
-                if (fresh && (m & lanemask_lt()) == 0) atomicAdd(&pc[panel], (uint32_t)__popc(m));
+            for (uint32_t c0 = 0; c0 < total; c0 += kSymThreads * kSymItems) {
+                // blocked: thread t takes products [c0 + t*kSymItems, ... + kSymItems)
+                const uint32_t q0 = c0 + t * kSymItems;
+                uint32_t kk = 0;
+                if (q0 < total) {
+                    uint32_t hi = kSymThreads;
+                    while (hi - kk > 1) {
+                        const uint32_t mid = (kk + hi) >> 1;
+                        if (wscan[mid] <= q0) kk = mid; else hi = mid;
+                    }
+                }
+#pragma unroll
+                for (int i = 0; i < kSymItems; ++i) {
+                    const uint32_t q = q0 + i;
+                    uint32_t panel = 0xffffffffu;
+                    if (q < total) {
+                        while (kk + 1 < kSymThreads && wscan[kk] + wl[kk] <= q) ++kk;
+                        const uint32_t col = op.b_col[ws[kk] + (q - wscan[kk])];
+                        const uint32_t bit = 1u << (col & 31);
+                        const uint32_t old = atomicOr(&bits[col >> 5], bit);
+                        if (!(old & bit)) panel = col >> op.panel_log2;
+                    }
+                    const uint32_t m = __match_any_sync(kFullMask, panel);
+                    if (panel != 0xffffffffu && (m & lanemask_lt()) == 0) atomicAdd(&pc[panel], (uint32_t)__popc(m));
+                }
             }
             __syncthreads();
         }
@@ -285,39 +315,62 @@ void launch_sym_bitmap(const Operands& op, const uint32_t* rows, uint32_t nrows,
 }
 
 // ---------------------------------------------------------------------------------------------
-// numeric pass for the other rows: one block per part (a row's columns in fine panels
-// [p0, p1)), open-addressing table of kHashSlots in shared memory
+// numeric pass for the other rows: one block per part (a row's columns in fine panels [p0, p1)).
+// A dense part indexes its accumulator by column directly; a sparse part uses an open-addressing
+// table.  Both live in the same shared-memory region.
+//
+// The part's products are processed in segments of at most kSeg products, in stream order.  A
+// segment inside one A nonzero needs no ordering (its columns are distinct), and consecutive
+// segments of the same A nonzero need no barrier either.  A segment spanning several short A
+// nonzeros applies each column's products in stream order through claim rounds.
 // ---------------------------------------------------------------------------------------------
 
-constexpr int kHashThreads = 512;
-constexpr int kHashItems = 4;                          // products per thread per chunk
-constexpr int kChunk = kHashThreads * kHashItems;      // 2048 products
-constexpr uint32_t kHashSlots = 8192;
-constexpr uint32_t kClaimCells = 2048;
+constexpr int kPartThreads = 512;
+constexpr int kPartWarps = kPartThreads / 32;
+constexpr int kItems = 4;                              // products per thread per segment
+constexpr int kSeg = kPartThreads * kItems;            // 2048 products
+constexpr uint32_t kHashSlots = 8192;                  // sparse part: vals[8192] + keys[8192]
+constexpr uint32_t kDenseCols = 12288;                 // dense part: vals[12288] (same 96 KiB)
+constexpr uint32_t kClaimCells = 1024;
 constexpr uint32_t kNoClaim = 0xffffffffu;
+constexpr uint32_t kLongK = 256;                       // an A nonzero with this many products left
+                                                       // gets segments of its own
+constexpr size_t kRegionBytes = (size_t)kHashSlots * (sizeof(double) + sizeof(uint32_t));
+static_assert(kRegionBytes == kDenseCols * sizeof(double), "dense and sparse layouts share one region");
 
 uint32_t hash_part_capacity() { return kHashSlots * 3 / 4; }  // load factor <= 0.75
+uint32_t hash_part_min_bits() { return 9; }                    // 512 slots: 32 per warp
+uint32_t dense_part_columns() { return kDenseCols; }
 
-__global__ void __launch_bounds__(kHashThreads, 2)
+// largest k in [lo, kPartThreads) with wscan[k] <= q (zero-length nonzeros share the next one's
+// start, so this is the nonzero holding product q)
+__device__ __forceinline__ uint32_t find_nonzero(const uint32_t* wscan, uint32_t lo, uint32_t q) {
+    uint32_t hi = kPartThreads;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (wscan[mid] <= q) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(kPartThreads, 2)
     hash_part_kernel(Operands op, const PartItem* __restrict__ parts, uint32_t nparts, OutputView out,
                      uint32_t* __restrict__ work_counter, uint32_t* __restrict__ overflow) {
     extern __shared__ __align__(16) unsigned char smem[];
-    double* vals = reinterpret_cast<double*>(smem);                               // [kHashSlots]
-    uint32_t* keys = reinterpret_cast<uint32_t*>(vals + kHashSlots);              // [kHashSlots]
-    uint32_t* claim = keys + kHashSlots;                                          // [kClaimCells]
-    __shared__ double wa[kHashThreads];
-    __shared__ uint32_t ws[kHashThreads], wl[kHashThreads], wscan[kHashThreads];
-    __shared__ uint32_t tmp[kHashThreads / 32 + 1];
-    __shared__ uint32_t wtot[kHashThreads / 32];
+    double* vals = reinterpret_cast<double*>(smem);                                    // region
+    uint32_t* keys = reinterpret_cast<uint32_t*>(smem + kHashSlots * sizeof(double));  // sparse layout
+    uint32_t* claim = reinterpret_cast<uint32_t*>(smem + kRegionBytes);               // [kClaimCells]
+    __shared__ double wa[kPartThreads];
+    __shared__ uint32_t ws[kPartThreads], wl[kPartThreads], wscan[kPartThreads], nxt[kPartThreads];
+    __shared__ uint32_t tmp[kPartWarps + 1];
+    __shared__ uint32_t wtot[kPartWarps];
     __shared__ uint32_t s_item;
+    __shared__ uint64_t s_base;
     const uint32_t t = threadIdx.x, lane = lane_id(), warp = t >> 5;
-    constexpr uint32_t kWarps = kHashThreads / 32;
+    unsigned long long* vbits = reinterpret_cast<unsigned long long*>(vals);
 
-    for (uint32_t i = t; i < kHashSlots; i += kHashThreads) {
-        keys[i] = kEmptyCol;
-        reinterpret_cast<unsigned long long*>(vals)[i] = kNoValue;
-    }
-    for (uint32_t i = t; i < kClaimCells; i += kHashThreads) claim[i] = kNoClaim;
+    for (uint32_t i = t; i < kClaimCells; i += kPartThreads) claim[i] = kNoClaim;
+    int layout = -1;  // 0 sparse, 1 dense (uniform)
 
     for (;;) {
         __syncthreads();
@@ -326,11 +379,26 @@ __global__ void __launch_bounds__(kHashThreads, 2)
         const uint32_t item = s_item;
         if (item >= nparts) break;
         const PartItem it = parts[item];
+        const bool dense = (it.mode & 1u) != 0;
+        const uint32_t tmask = dense ? 0u : (1u << (it.mode >> 1)) - 1u;
         const uint32_t row = it.row;
+        const uint32_t lo = it.p0 << op.panel_log2;  // first column of the part
+        if ((int)dense != layout) {
+            if (dense) {
+                for (uint32_t i = t; i < kDenseCols; i += kPartThreads) vbits[i] = kNoValue;
+            } else {
+                for (uint32_t i = t; i < kHashSlots; i += kPartThreads) {
+                    vbits[i] = kNoValue;
+                    keys[i] = kEmptyCol;
+                }
+            }
+            layout = dense;
+            __syncthreads();
+        }
         const uint32_t ka = op.row_start[row], kb = op.row_start[row + 1];
-        bool full = false;  // table overflow (only possible with an underestimated size)
+        bool bad = false;  // table overflow or a column outside a dense part (never for exact sizes)
 
-        for (uint32_t kw = ka; kw < kb; kw += kHashThreads) {
+        for (uint32_t kw = ka; kw < kb; kw += kPartThreads) {
             const uint32_t k = kw + t;
             uint32_t L = 0, s = 0;
             double a = 0.0;
@@ -344,81 +412,123 @@ __global__ void __launch_bounds__(kHashThreads, 2)
                 }
             }
             uint32_t total;
-            const uint32_t excl = block_exclusive_scan<uint32_t, kHashThreads>(L, tmp, &total);
+            const uint32_t excl = block_exclusive_scan<uint32_t, kPartThreads>(L, tmp, &total);
             ws[t] = s;
             wl[t] = L;
             wscan[t] = excl;
             wa[t] = a;
+            // nxt[k] = first nonzero >= k in this window with at least kLongK products
+            {
+                const uint32_t longmask = __ballot_sync(kFullMask, L >= kLongK);
+                if (lane == 0) tmp[warp] = longmask;  // free again: the scan has finished with it
+                __syncthreads();
+                const uint32_t m = longmask & ~lanemask_lt();
+                uint32_t n = kPartThreads;
+                if (m) {
+                    n = warp * 32 + __ffs(m) - 1;
+                } else {
+                    for (uint32_t w2 = warp + 1; w2 < kPartWarps; ++w2)
+                        if (tmp[w2]) { n = w2 * 32 + __ffs(tmp[w2]) - 1; break; }
+                }
+                nxt[t] = n;
+            }
             __syncthreads();
 
-            uint32_t kcur = 0;   // uniform: A nonzero holding the chunk's first product
-            uint32_t kk = 0;     // per thread cursor
-            for (uint32_t c0 = 0; c0 < total; c0 += kChunk) {
-                while (kcur + 1 < kHashThreads && wscan[kcur] + wl[kcur] <= c0) ++kcur;
-                const uint32_t cend = min(c0 + (uint32_t)kChunk, total);
-                const bool single = wscan[kcur] + wl[kcur] >= cend;
-                uint32_t slot[kHashItems];
-                double prod[kHashItems];
-                uint32_t col[kHashItems];
-                if (kk < kcur) kk = kcur;
+            uint32_t pos = 0;
+            while (pos < total) {
+                const uint32_t kcur = find_nonzero(wscan, 0, pos);  // uniform
+                const uint32_t kend = wscan[kcur] + wl[kcur];
+                uint32_t seg_end;
+                if (kend - pos >= kLongK) {
+                    seg_end = min(pos + (uint32_t)kSeg, kend);
+                } else {
+                    const uint32_t nl = (kcur + 1 < kPartThreads) ? nxt[kcur + 1] : kPartThreads;
+                    const uint32_t stop = nl < kPartThreads ? wscan[nl] : total;
+                    seg_end = min(min(pos + (uint32_t)kSeg, total), max(stop, kend));
+                }
+                const bool single = seg_end <= kend;
+                uint32_t col[kItems];
+                uint32_t slot[kItems];
+                double prod[kItems];
+                if (single) {
+                    // strided: consecutive threads read consecutive fiber entries
+                    const int64_t jb = (int64_t)ws[kcur] - (int64_t)wscan[kcur];
+                    const double ak = wa[kcur];
 #pragma unroll
-                for (int i = 0; i < kHashItems; ++i) {
-                    const uint32_t p = c0 + i * kHashThreads + t;
-                    col[i] = kEmptyCol;
-                    prod[i] = 0.0;
-                    if (p < total) {
-                        while (kk + 1 < kHashThreads && wscan[kk] + wl[kk] <= p) ++kk;
-                        const uint32_t j = ws[kk] + (p - wscan[kk]);
-                        col[i] = op.b_col[j];
-                        prod[i] = __dmul_rn(wa[kk], op.b_val[j]);
+                    for (int i = 0; i < kItems; ++i) {
+                        const uint32_t q = pos + i * kPartThreads + t;
+                        col[i] = kEmptyCol;
+                        prod[i] = 0.0;
+                        if (q < seg_end) {
+                            const uint32_t j = (uint32_t)(jb + q);
+                            col[i] = op.b_col[j];
+                            prod[i] = __dmul_rn(ak, op.b_val[j]);
+                        }
+                    }
+                } else {
+                    // blocked: thread t takes products [pos + t*kItems, ... + kItems)
+                    const uint32_t q0 = pos + t * kItems;
+                    uint32_t kk = q0 < seg_end ? find_nonzero(wscan, kcur, q0) : kcur;
+#pragma unroll
+                    for (int i = 0; i < kItems; ++i) {
+                        const uint32_t q = q0 + i;
+                        col[i] = kEmptyCol;
+                        prod[i] = 0.0;
+                        if (q < seg_end) {
+                            while (kk + 1 < kPartThreads && wscan[kk] + wl[kk] <= q) ++kk;
+                            const uint32_t j = ws[kk] + (q - wscan[kk]);
+                            col[i] = op.b_col[j];
+                            prod[i] = __dmul_rn(wa[kk], op.b_val[j]);
+                        }
                     }
                 }
-                // find or insert every product's column (concurrent inserts of distinct keys are safe)
+                // accumulator slot of every product
 #pragma unroll
-                for (int i = 0; i < kHashItems; ++i) {
+                for (int i = 0; i < kItems; ++i) {
                     slot[i] = kEmptyCol;
-                    if (col[i] != kEmptyCol) {
-                        uint32_t h = hash32(col[i]) & (kHashSlots - 1);
-                        for (uint32_t probe = 0; probe < kHashSlots; ++probe) {
+                    if (col[i] == kEmptyCol) continue;
+                    if (dense) {
+                        const uint32_t d = col[i] - lo;
+                        if (d < kDenseCols) slot[i] = d;
+                    } else {
+                        uint32_t h = hash32(col[i]) & tmask;
+                        for (uint32_t probe = 0; probe <= tmask; ++probe) {
                             const uint32_t cur = keys[h];
                             if (cur == col[i]) { slot[i] = h; break; }
                             if (cur == kEmptyCol) {
                                 const uint32_t old = atomicCAS(&keys[h], kEmptyCol, col[i]);
                                 if (old == kEmptyCol || old == col[i]) { slot[i] = h; break; }
                             }
-                            h = (h + 1) & (kHashSlots - 1);
+                            h = (h + 1) & tmask;
                         }
-                        if (slot[i] == kEmptyCol) { full = true; col[i] = kEmptyCol; }
                     }
+                    if (slot[i] == kEmptyCol) { bad = true; col[i] = kEmptyCol; }
                 }
                 if (single) {
-                    // one A nonzero: every column distinct, no ordering needed
 #pragma unroll
-                    for (int i = 0; i < kHashItems; ++i)
+                    for (int i = 0; i < kItems; ++i)
                         if (col[i] != kEmptyCol) accumulate(&vals[slot[i]], prod[i]);
-                    // the next chunk may start another A nonzero that meets these columns
-                    const uint32_t nend = min(cend + (uint32_t)kChunk, total);
-                    const bool next_same = cend < total && wscan[kcur] + wl[kcur] >= nend;
-                    if (!next_same) __syncthreads();
+                    pos = seg_end;
+                    if (pos == kend) __syncthreads();  // the next segment starts another A nonzero
                 } else {
                     // several A nonzeros: per column, apply in stream order (claim rounds)
                     __syncthreads();
-                    bool pending[kHashItems];
+                    bool pending[kItems];
 #pragma unroll
-                    for (int i = 0; i < kHashItems; ++i) pending[i] = col[i] != kEmptyCol;
-                    for (uint32_t round = 0; round < (uint32_t)kChunk + 1; ++round) {
+                    for (int i = 0; i < kItems; ++i) pending[i] = col[i] != kEmptyCol;
+                    for (uint32_t round = 0; round < (uint32_t)kSeg + 1; ++round) {
 #pragma unroll
-                        for (int i = 0; i < kHashItems; ++i)
-                            if (pending[i]) atomicMin(&claim[slot[i] & (kClaimCells - 1)], i * kHashThreads + t);
+                        for (int i = 0; i < kItems; ++i)
+                            if (pending[i]) atomicMin(&claim[slot[i] & (kClaimCells - 1)], t * kItems + i);
                         __syncthreads();
-                        bool mine[kHashItems];
+                        bool mine[kItems];
 #pragma unroll
-                        for (int i = 0; i < kHashItems; ++i)
-                            mine[i] = pending[i] && claim[slot[i] & (kClaimCells - 1)] == i * kHashThreads + t;
+                        for (int i = 0; i < kItems; ++i)
+                            mine[i] = pending[i] && claim[slot[i] & (kClaimCells - 1)] == t * kItems + i;
                         __syncthreads();
                         bool left = false;
 #pragma unroll
-                        for (int i = 0; i < kHashItems; ++i) {
+                        for (int i = 0; i < kItems; ++i) {
                             if (mine[i]) {
                                 accumulate(&vals[slot[i]], prod[i]);
                                 claim[slot[i] & (kClaimCells - 1)] = kNoClaim;
@@ -428,32 +538,51 @@ __global__ void __launch_bounds__(kHashThreads, 2)
                         }
                         if (!__syncthreads_or(left)) break;
                     }
+                    pos = seg_end;
                 }
             }
             __syncthreads();
         }
-        if (__syncthreads_or(full)) {
-            if (t == 0) atomicOr(overflow, 1u);
-        }
+        const bool any_bad = __syncthreads_or(bad);
 
-        // emit in slot order: warp w owns slots [w * span, (w + 1) * span)
-        constexpr uint32_t span = kHashSlots / kWarps;
+        // emit: warp w owns slots [w * span, (w + 1) * span); dense parts come out in column order
+        const uint32_t span = (dense ? kDenseCols : tmask + 1) / kPartWarps;
         uint32_t cnt = 0;
         for (uint32_t i = 0; i < span; i += 32)
-            cnt += __popc(__ballot_sync(kFullMask, keys[warp * span + i + lane] != kEmptyCol));
+            cnt += __popc(__ballot_sync(kFullMask, vbits[warp * span + i + lane] != kNoValue));
         if (lane == 0) wtot[warp] = cnt;
         __syncthreads();
-        uint64_t o = it.out_off;
+        if (t == 0) {
+            uint64_t base = it.out_off, total = 0;
+            for (uint32_t w = 0; w < kPartWarps; ++w) total += wtot[w];
+            if (base == kClaimOffset) {
+                base = any_bad ? ~0ull : claim_output(out, total);
+                if (base == ~0ull) {  // rerun this part exactly
+                    const uint32_t f = atomicAdd(out.fail_count, 1u);
+                    out.fail_list[f] = item;
+                }
+            } else if (any_bad) {
+                atomicOr(overflow, 1u);  // exact sizes cannot overflow: report an internal error
+                base = ~0ull;
+            }
+            if (out.item_count) out.item_count[item] = base == ~0ull ? 0u : (uint32_t)total;
+            s_base = base;
+        }
+        __syncthreads();
+        const uint64_t base = s_base;
+        uint64_t o = base;
         for (uint32_t w = 0; w < warp; ++w) o += wtot[w];
         for (uint32_t i = 0; i < span; i += 32) {
             const uint32_t sidx = warp * span + i + lane;
-            const uint32_t kc = keys[sidx];
-            const bool occ = kc != kEmptyCol;
+            const bool occ = vbits[sidx] != kNoValue;
             const uint32_t m = __ballot_sync(kFullMask, occ);
             if (occ) {
-                write_entry(op, out, o + __popc(m & lanemask_lt()), row, kc, vals[sidx]);
-                keys[sidx] = kEmptyCol;
-                reinterpret_cast<unsigned long long*>(vals)[sidx] = kNoValue;
+                if (base != ~0ull) {
+                    const uint32_t c = dense ? lo + sidx : keys[sidx];
+                    write_entry(op, out, o + __popc(m & lanemask_lt()), row, c, vals[sidx]);
+                }
+                vbits[sidx] = kNoValue;
+                if (!dense) keys[sidx] = kEmptyCol;
             }
             o += __popc(m);
         }
@@ -463,14 +592,14 @@ __global__ void __launch_bounds__(kHashThreads, 2)
 void launch_hash_parts(const Operands& op, const PartItem* parts, uint32_t nparts, const OutputView& out,
                        uint32_t* work_counter, uint32_t* overflow, int num_sms, cudaStream_t st) {
     if (nparts == 0) return;
-    const size_t smem = (size_t)kHashSlots * (sizeof(double) + sizeof(uint32_t)) + kClaimCells * sizeof(uint32_t);
+    const size_t smem = kRegionBytes + kClaimCells * sizeof(uint32_t);
     PTC_CUDA(cudaMemsetAsync(work_counter, 0, sizeof(uint32_t), st));
     PTC_CUDA(cudaFuncSetAttribute(hash_part_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 1;
-    PTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hash_part_kernel, kHashThreads, smem));
+    PTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hash_part_kernel, kPartThreads, smem));
     per_sm = per_sm < 1 ? 1 : per_sm;
     const uint32_t grid = (uint32_t)std::min<uint64_t>(nparts, (uint64_t)num_sms * per_sm);
-    hash_part_kernel<<<grid, kHashThreads, smem, st>>>(op, parts, nparts, out, work_counter, overflow);
+    hash_part_kernel<<<grid, kPartThreads, smem, st>>>(op, parts, nparts, out, work_counter, overflow);
     count_launch();
     PTC_CHECK_LAUNCH();
 }

@@ -7,8 +7,12 @@ namespace ptc {
 
 // rows with at most this many products go to the one-warp-per-row kernel
 uint32_t small_row_max_flops();
-// largest exact output count one hash part may hold
+// largest exact output count one open-addressing part may hold
 uint32_t hash_part_capacity();
+// column width of a dense (direct-mapped) part
+uint32_t dense_part_columns();
+// smallest open-addressing table (log2 slots) a part uses
+uint32_t hash_part_min_bits();
 // largest column count the bitmap symbolic pass handles
 uint32_t sym_bitmap_max_cols();
 
@@ -27,18 +31,44 @@ void launch_hash_parts(const Operands& op, const PartItem* parts, uint32_t npart
 
 // ---- planning (ptc_plan.cu) ----
 
-// class_of[r]: 0 = no products, 1 = small, 2 = other; flags for the two compactions
-void launch_classify_rows(const uint64_t* row_flops, uint64_t nrows, uint64_t small_max, uint32_t* small_flag,
-                          uint32_t* big_flag, cudaStream_t st);
+// Row classes: no products (skipped), small (<= small_max products: one warp), sort-based
+// (fewer than esc_avg products per A nonzero on average), other (block hash).  One flag array
+// per class for the compactions.
+void launch_classify_rows(const uint64_t* row_flops, const uint32_t* row_start, uint64_t nrows, uint64_t small_max,
+                          uint32_t esc_avg, uint32_t* small_flag, uint32_t* big_flag, uint32_t* esc_flag,
+                          cudaStream_t st);
+// big_flag[r] |= esc_flag[r] (sort-based rows fall back to the hash path)
+void launch_merge_flags(uint32_t* big_flag, const uint32_t* esc_flag, uint64_t nrows, cudaStream_t st);
+
+// ---- sort-based rows (ptc_esc.cu) ----
+void launch_esc_index(const uint32_t* esc_rows, uint64_t n, int32_t* esc_of, cudaStream_t st);
+void launch_esc_len(const uint32_t* esc_rows, uint64_t n, const uint64_t* row_flops, uint64_t* len, cudaStream_t st);
+void launch_esc_expand(const Operands& op, const uint32_t* a_row, const int32_t* esc_of, const uint64_t* poff,
+                       const uint64_t* esc_off, uint32_t colbits, uint64_t* key, double* val, uint32_t* perm,
+                       cudaStream_t st);
+void launch_esc_count(const uint64_t* run_key, uint64_t nruns, uint32_t colbits, const uint32_t* esc_rows,
+                      uint64_t* row_d, uint32_t* first_run, cudaStream_t st);
+void launch_esc_fold(const Operands& op, const OutputView& out, const uint64_t* run_key, const uint32_t* run_start,
+                     uint64_t nruns, uint32_t colbits, const uint32_t* esc_rows, const uint32_t* first_run,
+                     const uint64_t* row_off, const uint32_t* perm, const double* val, uint64_t nprod,
+                     double* sorted, cudaStream_t st);
 // out[pos[i]] = i wherever flag[i] (pos = exclusive scan of flag)
 void launch_compact_indices(const uint32_t* flag, const uint32_t* pos, uint64_t n, uint32_t* out, cudaStream_t st);
 // key[i] = ~row_flops[rows[i]] (descending-work sort key)
 void launch_work_keys(const uint32_t* rows, uint64_t n, const uint64_t* row_flops, uint64_t* key, cudaStream_t st);
-// number of parts of each big row under the capacity (greedy over fine panels, in order);
-// sets *oversize if one fine panel alone exceeds the capacity
-void launch_count_parts(const uint32_t* panel_cnt, uint64_t nbig, uint32_t npanels, uint32_t cap, uint32_t* nparts,
+// How a large row is cut into parts, from its exact output count per fine panel: windows of
+// dense_panels panels holding at least dense_min entries per panel become dense parts; the
+// other panels are grouped greedily into open-addressing parts of at most cap entries.
+struct SplitRule {
+    uint32_t cap;
+    uint32_t dense_panels;  // 0 disables dense parts
+    uint32_t dense_min;
+    uint32_t min_bits;      // smallest open-addressing table, log2 slots
+};
+// number of parts of each big row; sets *oversize if one fine panel alone exceeds cap
+void launch_count_parts(const uint32_t* panel_cnt, uint64_t nbig, uint32_t npanels, SplitRule rule, uint32_t* nparts,
                         uint32_t* oversize, cudaStream_t st);
-void launch_fill_parts(const uint32_t* rows, const uint32_t* panel_cnt, uint64_t nbig, uint32_t npanels, uint32_t cap,
+void launch_fill_parts(const uint32_t* rows, const uint32_t* panel_cnt, uint64_t nbig, uint32_t npanels, SplitRule rule,
                        const uint32_t* part_pos, const uint64_t* row_off, PartItem* parts, cudaStream_t st);
 
 }  // namespace ptc

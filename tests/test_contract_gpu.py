@@ -37,7 +37,7 @@ CASES = [
 
 
 @pytest.mark.parametrize("case", CASES, ids=[f"c{i}" for i in range(len(CASES))])
-@pytest.mark.parametrize("panel", [0, 256])
+@pytest.mark.parametrize("panel", [0, 64, 4096])
 def test_against_oracle(engine, oracle_mod, case, panel):
     dims, nnz, alphas, seed, values, c, modes = case
     t = gen.random_coo(dims, nnz, alphas, seed, values)
