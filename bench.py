@@ -39,13 +39,6 @@ WORKLOAD = "zipf4d_3m"
 FALLBACK_HBM_GBS = 6650.0
 
 
-def _env_int(name, default):
-    try:
-        return int(os.environ.get(name, default))
-    except ValueError:
-        return default
-
-
 class ClockSampler:
     """nvidia-smi SM clock / throttle-reason samples while the timed region runs."""
 
@@ -176,10 +169,13 @@ def cpu_arm(w, target_flops, steps, warmup):
                 times.append(r["t_wall"])
     t = statistics.median(times)
     value = sflops / t
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)) if kind == "reference" else 1
+    # the reference is offered every host core (OMP_NUM_THREADS), but its hash builds are serial
+    # loops and its numeric loop runs a team of one (fksCuckooTC.hpp:171-173): one core works
+    cores = 1
     sample = (f"{nrows} of A's rows (whole rows, seeded) against the whole B: {sflops} mult-adds; time = the "
               f"reference's HT_B + HT_A builds, preprocessing and numeric pass; median of {len(times)}; "
-              f"the reference runs its numeric loop on 1 thread (fksCuckooTC.hpp:171-173)")
+              f"OMP_NUM_THREADS={os.cpu_count()} offered, the reference's loops use one thread "
+              f"(fksCuckooTC.hpp:171-173)")
     return value, {"value": value, "unit": "mult-adds/s", "cores": cores, "kind": kind, "sample": sample,
                    "sample_mult_adds": sflops, "seconds": t}
 
@@ -202,16 +198,15 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
-    rank = _env_int("RANK", 0)
-    world = _env_int("WORLD_SIZE", 1)
-    local = _env_int("LOCAL_RANK", 0)
+    from partc_b200 import dist as pdist
+    rank, world, local = pdist.rank_env()
 
     from partc_b200 import gen
     w = gen.WORKLOADS[args.workload]()
     t = w.tensor
 
     if args.impl == "reference":
-        if rank != 0:
+        if not pdist.runs_reference_arm(rank):
             return
         steps = max(1, args.steps)
         value, cb = cpu_arm(w, int(args.cpu_target_flops / 2), steps, min(args.warmup, 1))
@@ -232,8 +227,7 @@ def main():
 
     torch.cuda.set_device(local)
     if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+        pdist.init("nccl", local)
 
     stream = torch.cuda.Stream()
     di = torch.from_numpy(t.idx.view(np.int32)).to(f"cuda:{local}")
@@ -250,8 +244,7 @@ def main():
     for _ in range(args.warmup):
         st0 = step()
     torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+    pdist.barrier()
     torch.cuda.synchronize()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
@@ -262,17 +255,12 @@ def main():
             stats.append(step())
         ev1.record(stream)
         torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+    pdist.barrier()
     torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
-    if world > 1:
-        tt = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = pdist.max_over_ranks(ev0.elapsed_time(ev1), device=f"cuda:{local}")
     M = stats[0]["mult_adds"]
     R = stats[0]["out_nnz"]
-    value = world * args.steps * M / (ms * 1e-3)
+    value = pdist.job_throughput(M, args.steps, world, ms * 1e-3)
     ms_step = ms / args.steps
 
     # numeric pass roofline
@@ -295,19 +283,15 @@ def main():
         pv = torch.from_numpy(t.vals).pin_memory()
         ht = CooTensor(idx=pi.numpy().view(np.uint32), vals=pv.numpy(), dims=t.dims)
         e2e_opts = dict(device=local, stream=stream.cuda_stream, path=args.path)
-        _lib.contract(ht, None, w.c, w.modes, **e2e_opts)  # warm-up
-        if world > 1:
-            dist.barrier()
+        idx, vals, _ = _lib.contract(ht, None, w.c, w.modes, **e2e_opts)  # warm-up
+        del idx, vals
+        pdist.barrier()
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
             idx, vals, _ = _lib.contract(ht, None, w.c, w.modes, **e2e_opts)
             del idx, vals
-        el = time.perf_counter() - t0
-        if world > 1:
-            tt = torch.tensor([el], device=f"cuda:{local}", dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            el = float(tt.item())
-        e2e = {"value": world * args.e2e_steps * M / el, "unit": "mult-adds/s",
+        el = pdist.max_over_ranks(time.perf_counter() - t0, device=f"cuda:{local}")
+        e2e = {"value": pdist.job_throughput(M, args.e2e_steps, world, el), "unit": "mult-adds/s",
                "h2d_bytes_per_step": t.nnz * (4 * t.order + 8), "d2h_bytes_per_step": R * (4 * od + 8),
                "steps": args.e2e_steps, "ms_per_step": el / args.e2e_steps * 1e3}
 

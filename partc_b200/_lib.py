@@ -190,13 +190,35 @@ def contract(A, B=None, c: int = 1, a_modes=None, b_modes=None, *, keep_device: 
     _check(rc)
     if o.output_location == PTC_DEVICE:
         return out, None, st.as_dict()
-    try:
-        n, d = out.nnz, out.order
-        idx = np.ctypeslib.as_array(out.idx, shape=(n * d,)).reshape(n, d).copy() if n else np.zeros((0, d), np.uint32)
-        vals = np.ctypeslib.as_array(out.vals, shape=(n,)).copy() if n else np.zeros(0, np.float64)
-    finally:
-        L.ptc_tensor_free(C.byref(out))
+    idx, vals = _host_arrays(out)
     return idx, vals, st.as_dict()
+
+
+class _Owner:
+    """Releases a host ptc_tensor when the last numpy view of it is gone."""
+
+    def __init__(self, t: Tensor):
+        self.t = t
+
+    def __del__(self):
+        if _lib is not None:
+            _lib.ptc_tensor_free(C.byref(self.t))
+
+
+def _host_arrays(out: Tensor):
+    """Zero-copy numpy views of a host output tensor (the views own it)."""
+    n, d = out.nnz, out.order
+    if n == 0:
+        lib().ptc_tensor_free(C.byref(out))
+        return np.zeros((0, d), np.uint32), np.zeros(0, np.float64)
+    owner = _Owner(out)
+    ib = (C.c_uint32 * (n * d)).from_address(C.addressof(out.idx.contents))
+    vb = (C.c_double * n).from_address(C.addressof(out.vals.contents))
+    ib._owner = owner
+    vb._owner = owner
+    idx = np.frombuffer(ib, dtype=np.uint32).reshape(n, d)
+    vals = np.frombuffer(vb, dtype=np.float64)
+    return idx, vals
 
 
 def contract_coo(ca: Coo, cb: Optional[Coo], c: int, a_modes, b_modes=None, **opt):
