@@ -205,6 +205,17 @@ ptc_status ptc_sizer_train(ptc_sizer* s, const float* features, const float* tar
 /* out[i] = predicted log2(1 + output nnz) for n feature rows (host arrays). */
 ptc_status ptc_sizer_predict(const ptc_sizer* s, const float* features, uint64_t n, int32_t device,
                              float* out);
+/* ptc_sizer_predict without any device allocation.  No counterpart in the reference: it is for
+ * callers that cannot allocate device memory where they need a prediction (another allocator
+ * owns the device, or an allocation would synchronize the device or is not allowed there).  Its
+ * device scratch -- the BF16 weights, up to 65536 staged feature rows and their predictions -- is
+ * one static device array of about 4.3 MiB that every device loading the library keeps until the
+ * process exits.  n > 65536 is rejected with PTC_ERR_INVALID_ARGUMENT.  The first call on a device
+ * looks up that array's address; make it before capturing any stream.  All calls share the array:
+ * calls whose GPU work overlaps race on it.  Runs on the calling thread's per-thread default
+ * stream and returns when out holds the predictions (host arrays in and out). */
+ptc_status ptc_sizer_predict_noalloc(const ptc_sizer* s, const float* features, uint64_t n,
+                                     int32_t device, float* out);
 /* Gradient of the mean squared error over n samples (host arrays; grads has PTC_SIZER_PARAMS). */
 ptc_status ptc_sizer_gradients(const ptc_sizer* s, const float* features, const float* targets,
                                uint64_t n, int32_t device, float* grads, float* loss);

@@ -31,6 +31,7 @@ EXPORTS = [
     "ptc_tensor_free", "ptc_device_count", "ptc_train_options_init", "ptc_sizer_create", "ptc_sizer_load",
     "ptc_sizer_save", "ptc_sizer_free", "ptc_sizer_get_params", "ptc_sizer_set_params", "ptc_sizer_collect",
     "ptc_sizer_train", "ptc_sizer_predict", "ptc_sizer_gradients", "ptc_buffer_free",
+    "ptc_sizer_predict_noalloc",
 ]
 SIZER_FEATURES = 16
 SIZER_PARAMS = 5313
@@ -126,11 +127,12 @@ def lib():
         L.ptc_sizer_predict.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int32, C.c_void_p]
         L.ptc_sizer_gradients.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_int32, C.c_void_p,
                                           P(F)]
+        L.ptc_sizer_predict_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int32, C.c_void_p]
         L.ptc_buffer_free.argtypes = [C.c_void_p]
         L.ptc_buffer_free.restype = None
         for name in ("ptc_sizer_create", "ptc_sizer_load", "ptc_sizer_save", "ptc_sizer_get_params",
                      "ptc_sizer_set_params", "ptc_sizer_collect", "ptc_sizer_train", "ptc_sizer_predict",
-                     "ptc_sizer_gradients"):
+                     "ptc_sizer_gradients", "ptc_sizer_predict_noalloc"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -291,6 +293,13 @@ class Sizer:
         x = np.ascontiguousarray(x, dtype=np.float32)
         out = np.empty(x.shape[0], dtype=np.float32)
         _check(lib().ptc_sizer_predict(self.h, x.ctypes.data, x.shape[0], device, out.ctypes.data))
+        return out
+
+    def predict_noalloc(self, x: np.ndarray, device=-1) -> np.ndarray:
+        """Same as predict, through the entry point that allocates no device memory."""
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        out = np.empty(x.shape[0], dtype=np.float32)
+        _check(lib().ptc_sizer_predict_noalloc(self.h, x.ctypes.data, x.shape[0], device, out.ctypes.data))
         return out
 
     def gradients(self, x: np.ndarray, t: np.ndarray, device=-1):
