@@ -82,8 +82,9 @@ __global__ void esc_fold_kernel(Operands op, OutputView out, const uint64_t* __r
     if (r >= nruns) return;
     const uint64_t key = run_key[r];
     const uint32_t e = (uint32_t)(key >> colbits);
-    const uint32_t col = (uint32_t)(key & ((1ull << colbits) - 1));
     const uint32_t row = esc_rows[e];
+    uint32_t col = (uint32_t)(key & ((1ull << colbits) - 1));
+    if (op.row_colbase) col += op.row_colbase[row];  // item-local -> global column
     const uint32_t b = run_start[r], en = run_start[r + 1];
     double v = sorted[b];
     uint32_t i = b + 1;

@@ -47,6 +47,9 @@ struct Operands {
     uint32_t panel_log2 = 0;
     // set to nonzero by a kernel that met an impossible index (a bug guard: the access is skipped)
     uint32_t* err = nullptr;
+    // batches: column ids are local to each item; row_colbase[row] is the first global column of
+    // the row's item (null for a single contraction, where local and global ids coincide)
+    const uint32_t* row_colbase = nullptr;
 };
 
 // A part of a row for the hash accumulator: the row's columns in fine panels [p0, p1), and

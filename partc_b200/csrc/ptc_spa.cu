@@ -37,9 +37,11 @@ __device__ __forceinline__ void accumulate(double* slot, double p) {
     *slot = (__double_as_longlong(v) == (long long)kNoValue) ? p : __dadd_rn(v, p);
 }
 
-// Write output entry o = (row's A free tuple, column's B free tuple, value).
+// Write output entry o = (row's A free tuple, column's B free tuple, value); `col` is local to
+// the row's item.
 __device__ __forceinline__ void write_entry(const Operands& op, const OutputView& out, uint64_t o, uint32_t row,
                                             uint32_t col, double v) {
+    if (op.row_colbase) col += op.row_colbase[row];
     const uint32_t fa = op.fa, fb = op.fb, od = fa + fb;
     uint32_t* dst = out.idx + o * od;
     if (fa == 2 && fb == 2) {
@@ -57,6 +59,16 @@ __device__ __forceinline__ void write_entry(const Operands& op, const OutputView
 
 // Fiber entries of A nonzero k that fall in fine panels [p0, p1) (the whole fiber when the
 // column space is a single panel).
+// first entry of [lo, hi) (a fiber, sorted by column) whose column is >= c
+__device__ __forceinline__ uint32_t col_lower_bound(const uint32_t* __restrict__ col, uint32_t lo, uint32_t hi,
+                                                   uint32_t c) {
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (col[mid] < c) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
 __device__ __forceinline__ void part_range(const Operands& op, int32_t f, uint32_t p0, uint32_t p1, uint32_t& s,
                                            uint32_t& e) {
     if (op.panel_off) {
@@ -66,6 +78,10 @@ __device__ __forceinline__ void part_range(const Operands& op, int32_t f, uint32
     } else {
         s = op.fib_start[f];
         e = op.fib_start[f + 1];
+        if (op.npanels > 1) {  // no split table: search the fiber for the panels' columns
+            if (p0 > 0) s = col_lower_bound(op.b_col, s, e, p0 << op.panel_log2);
+            if (p1 < op.npanels) e = col_lower_bound(op.b_col, s, e, p1 << op.panel_log2);
+        }
     }
 }
 
