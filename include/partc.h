@@ -92,7 +92,15 @@ typedef struct ptc_options {
     const ptc_sizer* sizer;    /* PTC_PATH_LEARNED: trained sizer (NULL = built-in weights) */
     uint32_t sort_rows;        /* 1: rows of the output in increasing free-key order and every
                                   row in increasing column order (canonical COO) */
-    uint32_t reserved[7];
+    /* tuning knobs (0 = default) */
+    uint32_t small_max_products;    /* rows with at most this many products use the one-warp
+                                       accumulator (<= 512; default 512) */
+    uint32_t sort_max_avg_products; /* rows averaging fewer products per A nonzero use the
+                                       sort-based accumulator (default 32) */
+    uint32_t hash_load_pct;         /* cuckoo table load factor in percent, 10-90 (default 75) */
+    uint32_t batch_wave_mib;        /* ptc_batch_contract: device memory for one wave's outputs,
+                                       MiB (default: 60% of the free memory) */
+    uint32_t reserved[3];
 } ptc_options;
 
 /* Per-call statistics; every time is measured with CUDA events on the call's stream. */
@@ -119,7 +127,9 @@ typedef struct ptc_stats {
     uint64_t rerun_rows;       /* learned path: rows rerun exactly after an overflow */
     double sizer_mean_abs_log2_err; /* learned path: mean |log2(pred/actual)| over rows */
     uint64_t kernel_launches;  /* kernels this call launched */
-    double reserved[4];
+    uint64_t batch_waves;      /* ptc_batch_contract: output waves */
+    uint64_t rerun_items;      /* ptc_batch_contract, learned path: items rerun exactly */
+    double reserved[2];
 } ptc_stats;
 
 /* Fill *opt with defaults. */
@@ -155,6 +165,41 @@ ptc_status ptc_self_contract(const uint32_t* hedges, const double* vals, uint32_
 
 /* Release an output tensor made by this library. */
 void ptc_tensor_free(ptc_tensor* t);
+
+/* One contraction of a batch (no counterpart in the reference, which contracts one tensor per
+ * run).  A zeroed B (idx, dims NULL and nnz 0) means B = A with b_modes = a_modes: the
+ * self-contraction. */
+typedef struct ptc_batch_item {
+    ptc_coo A;
+    ptc_coo B;
+    uint32_t c;
+    uint32_t a_modes[16];
+    uint32_t b_modes[16];
+} ptc_batch_item;
+
+/* Receives item `item`'s output; the arrays are valid only during the call (the library reuses
+ * them) and must not be freed. */
+typedef void (*ptc_batch_sink)(void* user, uint32_t item, const ptc_tensor* out);
+
+/*
+ * Contract n independent items as one problem: every key of item i is offset into a key range of
+ * its own, so one pass of each kernel (keys, sorts, one cuckoo table, symbolic pass) serves the
+ * whole batch.  Outputs are produced in waves of consecutive items that fit opt->batch_wave_mib;
+ * each wave's numeric pass is one CUDA-graph launch.  Results of every item equal ptc_contract's
+ * (same entries; values bit-identical).
+ *   outs != NULL: outs[i] receives item i's output (release each with ptc_tensor_free; items of a
+ *                 wave share one block, freed with the last of them).  With PTC_DEVICE outputs
+ *                 every output stays on the device: one wave.
+ *   sink != NULL: sink(user, i, &view) is called for every item as its wave completes (views in
+ *                 opt->output_location memory, valid during the call only).
+ *   both NULL:    outputs are computed and discarded (for timing).
+ * Every input must be in the same memory.  Unlike ptc_contract, an item with no matching fiber or
+ * with at most one nonzero is not an error: its output is empty.  opt->path = PTC_PATH_LEARNED
+ * sizes the large rows with the sizer; an item whose prediction falls short runs again exactly.
+ * Replaces a loop of main.cpp:115-118 over many tensors.
+ */
+ptc_status ptc_batch_contract(const ptc_batch_item* items, uint32_t n, const ptc_options* opt,
+                              ptc_tensor* outs, ptc_batch_sink sink, void* user, ptc_stats* stats);
 
 /* Number of CUDA devices the library can use (sm_100 class). */
 int ptc_device_count(void);

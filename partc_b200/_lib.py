@@ -31,7 +31,7 @@ EXPORTS = [
     "ptc_tensor_free", "ptc_device_count", "ptc_train_options_init", "ptc_sizer_create", "ptc_sizer_load",
     "ptc_sizer_save", "ptc_sizer_free", "ptc_sizer_get_params", "ptc_sizer_set_params", "ptc_sizer_collect",
     "ptc_sizer_train", "ptc_sizer_predict", "ptc_sizer_gradients", "ptc_buffer_free",
-    "ptc_sizer_predict_noalloc",
+    "ptc_sizer_predict_noalloc", "ptc_batch_contract",
 ]
 SIZER_FEATURES = 16
 SIZER_PARAMS = 5313
@@ -58,7 +58,9 @@ class Options(C.Structure):
     _fields_ = [("struct_size", C.c_uint32), ("device", C.c_int32), ("stream", C.c_void_p),
                 ("path", C.c_uint32), ("output_location", C.c_uint32), ("verbose", C.c_uint32),
                 ("panel_width", C.c_uint32), ("hash_seed", C.c_uint64), ("sizer", C.c_void_p),
-                ("sort_rows", C.c_uint32), ("reserved", C.c_uint32 * 7)]
+                ("sort_rows", C.c_uint32), ("small_max_products", C.c_uint32),
+                ("sort_max_avg_products", C.c_uint32), ("hash_load_pct", C.c_uint32),
+                ("batch_wave_mib", C.c_uint32), ("reserved", C.c_uint32 * 3)]
 
 
 class Stats(C.Structure):
@@ -69,11 +71,20 @@ class Stats(C.Structure):
                 ("hash_attempts", C.c_uint32), ("panel_width", C.c_uint32),
                 ("rows_small", C.c_uint64), ("rows_hash", C.c_uint64), ("hash_parts", C.c_uint64),
                 ("rows_long", C.c_uint64), ("rerun_rows", C.c_uint64), ("sizer_mean_abs_log2_err", C.c_double),
-                ("kernel_launches", C.c_uint64), ("reserved", C.c_double * 4)]
+                ("kernel_launches", C.c_uint64), ("batch_waves", C.c_uint64), ("rerun_items", C.c_uint64),
+                ("reserved", C.c_double * 2)]
 
     def as_dict(self) -> dict:
         return {name: (getattr(self, name) if not name == "reserved" else None)
                 for name, _ in self._fields_ if name != "reserved"}
+
+
+class BatchItem(C.Structure):
+    _fields_ = [("A", Coo), ("B", Coo), ("c", C.c_uint32), ("a_modes", C.c_uint32 * 16),
+                ("b_modes", C.c_uint32 * 16)]
+
+
+SINK = C.CFUNCTYPE(None, C.c_void_p, C.c_uint32, C.POINTER(Tensor))
 
 
 class TrainOptions(C.Structure):
@@ -110,6 +121,9 @@ def lib():
         L.ptc_tensor_free.argtypes = [C.POINTER(Tensor)]
         L.ptc_tensor_free.restype = None
         L.ptc_device_count.restype = C.c_int
+        L.ptc_batch_contract.argtypes = [C.POINTER(BatchItem), C.c_uint32, C.POINTER(Options), C.POINTER(Tensor),
+                                         SINK, C.c_void_p, C.POINTER(Stats)]
+        L.ptc_batch_contract.restype = C.c_int
         P, F = C.POINTER, C.c_float
         L.ptc_train_options_init.argtypes = [P(TrainOptions)]
         L.ptc_train_options_init.restype = None
@@ -240,6 +254,53 @@ def contract_coo(ca: Coo, cb: Optional[Coo], c: int, a_modes, b_modes=None, **op
 
 def free(t: Tensor) -> None:
     lib().ptc_tensor_free(C.byref(t))
+
+
+def batch_items(work, keep: list, B_list=None):
+    """``BatchItem`` array for workloads with ``.tensor``, ``.c``, ``.modes`` (self-contractions),
+    or, where ``B_list[i]`` is given, ``(B tensor, b_modes)`` as item i's second operand."""
+    arr = (BatchItem * len(work))()
+    for i, w in enumerate(work):
+        it = arr[i]
+        it.A = _host_coo(w.tensor, keep)
+        it.c = w.c
+        for j, m in enumerate(w.modes):
+            it.a_modes[j] = m
+        if B_list is not None and B_list[i] is not None:
+            bt, bm = B_list[i]
+            it.B = _host_coo(bt, keep)
+            for j, m in enumerate(bm):
+                it.b_modes[j] = m
+    return arr
+
+
+def batch_contract(items, *, outputs: str = "arrays", sink=None, **opt):
+    """Run ``ptc_batch_contract`` on a ``BatchItem`` array.
+
+    outputs="arrays": returns ``(list of (idx, vals), stats)`` with host numpy arrays;
+    outputs="device": returns ``(list of Tensor, stats)`` kept on the device (free each);
+    outputs="sink":   calls ``sink(i, tensor)`` for every item (views valid during the call);
+    outputs="none":   discards the outputs (timing).
+    """
+    L = lib()
+    n = len(items)
+    if outputs == "device":
+        opt.setdefault("output_location", PTC_DEVICE)
+    o = options(**opt)
+    st = Stats()
+    outs = (Tensor * n)() if outputs in ("arrays", "device") else None
+    cb = SINK(0)
+    if outputs == "sink":
+        def _cb(user, i, t):
+            sink(int(i), t.contents)
+        cb = SINK(_cb)
+    rc = L.ptc_batch_contract(items, n, C.byref(o), outs, cb, None, C.byref(st))
+    _check(rc)
+    if outputs == "arrays":
+        return [_host_arrays(Tensor.from_buffer_copy(outs[i])) for i in range(n)], st.as_dict()
+    if outputs == "device":
+        return [outs[i] for i in range(n)], st.as_dict()
+    return None, st.as_dict()
 
 
 def device_count() -> int:

@@ -195,73 +195,82 @@ __device__ __forceinline__ uint32_t item_of(const uint64_t* __restrict__ off, ui
     return lo;
 }
 
-__global__ void pack_items_kernel(const uint32_t* __restrict__ idx, uint64_t nnz, const ItemSpec* __restrict__ specs,
-                                  const uint64_t* __restrict__ nnz_off, uint32_t nitems, int side,
-                                  uint64_t* __restrict__ key1, uint64_t* __restrict__ key2, uint32_t* __restrict__ err) {
+// Element i of the side's concatenation (item it, local nonzero i - off[it]): its contracted key
+// cbase + sum idx[mode[j]] * stride[j] over the contracted modes, its free key fbase + the same
+// over the free modes, and its value.
+__global__ void pack_items_kernel(const ItemSpec* __restrict__ specs, const uint64_t* __restrict__ off,
+                                  uint32_t nitems, int side, uint64_t nnz, uint64_t* __restrict__ ckey,
+                                  uint64_t* __restrict__ fkey, double* __restrict__ vals, uint32_t* __restrict__ err) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nnz) return;
-    const uint32_t it = item_of(nnz_off, nitems, i);
+    const uint32_t it = item_of(off, nitems, i);
     const ItemSide& s = specs[it].side[side];
     const uint32_t d = s.order;
-    const uint32_t* row = idx + s.idx_off + (i - nnz_off[it]) * d;
+    const uint64_t local = i - off[it];
+    const uint32_t* row = s.idx + local * d;
     uint32_t v[kMaxOrder];
     bool bad = false;
     for (uint32_t m = 0; m < d; ++m) {
         v[m] = row[m];
         bad |= v[m] >= s.dim[m];
     }
+    vals[i] = s.vals[local];
     if (bad) {
         atomicOr(err, 1u);
+        ckey[i] = 0;
+        fkey[i] = 0;
         return;
     }
     const uint32_t c = specs[it].c;
     uint64_t a = specs[it].cbase, b = s.fbase;
     for (uint32_t j = 0; j < c; ++j) a += (uint64_t)v[s.mode[j]] * s.stride[j];
     for (uint32_t j = c; j < d; ++j) b += (uint64_t)v[s.mode[j]] * s.stride[j];
-    key1[i] = a;
-    key2[i] = b;
+    ckey[i] = a;
+    fkey[i] = b;
 }
 
-void launch_pack_items(const uint32_t* idx, uint64_t nnz, const ItemSpec* specs, const uint64_t* nnz_off,
-                       uint32_t nitems, int side, uint64_t* ckey, uint64_t* fkey, uint32_t* err, cudaStream_t st) {
+void launch_pack_items(const ItemSpec* specs, const uint64_t* off, uint32_t nitems, int side, uint64_t nnz,
+                       uint64_t* ckey, uint64_t* fkey, double* vals, uint32_t* err, cudaStream_t st) {
     if (nnz == 0) return;
-    pack_items_kernel<<<ceil_div_u32(nnz, 256), 256, 0, st>>>(idx, nnz, specs, nnz_off, nitems, side, ckey, fkey, err);
+    pack_items_kernel<<<ceil_div_u32(nnz, 256), 256, 0, st>>>(specs, off, nitems, side, nnz, ckey, fkey, vals, err);
     count_launch();
     PTC_CHECK_LAUNCH();
 }
 
-// tuple[r * width + m] = free index m of run r's representative nonzero (zero past the item's
+// tuple[r * width + m] = free index m of run r's representative element (zero past the item's
 // own free-mode count)
-__global__ void item_tuples_kernel(const uint32_t* __restrict__ idx, const uint32_t* __restrict__ run_start,
-                                   const uint32_t* __restrict__ perm, uint64_t nruns,
-                                   const ItemSpec* __restrict__ specs, const uint64_t* __restrict__ nnz_off,
+__global__ void item_tuples_kernel(const uint32_t* __restrict__ run_start, const uint32_t* __restrict__ perm,
+                                   uint64_t nruns, const ItemSpec* __restrict__ specs, const uint64_t* __restrict__ off,
                                    uint32_t nitems, int side, uint32_t width, uint32_t* __restrict__ tuple) {
     const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= nruns) return;
     const uint64_t src = perm[run_start[r]];
-    const uint32_t it = item_of(nnz_off, nitems, src);
+    const uint32_t it = item_of(off, nitems, src);
     const ItemSide& s = specs[it].side[side];
     const uint32_t c = specs[it].c, nf = s.order - c;
-    const uint32_t* row = idx + s.idx_off + (src - nnz_off[it]) * s.order;
+    const uint32_t* row = s.idx + (src - off[it]) * s.order;
     for (uint32_t m = 0; m < width; ++m) tuple[r * width + m] = m < nf ? row[s.mode[c + m]] : 0u;
 }
 
-void launch_item_tuples(const uint32_t* idx, const uint32_t* run_start, const uint32_t* perm, uint64_t nruns,
-                        const ItemSpec* specs, const uint64_t* nnz_off, uint32_t nitems, int side, uint32_t width,
-                        uint32_t* tuple, cudaStream_t st) {
+void launch_item_tuples(const uint32_t* run_start, const uint32_t* perm, uint64_t nruns, const ItemSpec* specs,
+                        const uint64_t* off, uint32_t nitems, int side, uint32_t width, uint32_t* tuple,
+                        cudaStream_t st) {
     if (nruns == 0 || width == 0) return;
-    item_tuples_kernel<<<ceil_div_u32(nruns, 256), 256, 0, st>>>(idx, run_start, perm, nruns, specs, nnz_off, nitems,
-                                                                 side, width, tuple);
+    item_tuples_kernel<<<ceil_div_u32(nruns, 256), 256, 0, st>>>(run_start, perm, nruns, specs, off, nitems, side,
+                                                                 width, tuple);
     count_launch();
     PTC_CHECK_LAUNCH();
 }
 
-// first[i] = first index of sorted `keys` (n distinct, increasing) that is >= base[i]
+// first[i] = first index of the sorted `keys` that is >= base[i]; first[nitems] = n
 __global__ void key_bounds_kernel(const uint64_t* __restrict__ keys, uint64_t n, const uint64_t* __restrict__ base,
                                   uint32_t nitems, uint32_t* __restrict__ first) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i > nitems) return;
-    if (i == nitems) { first[i] = (uint32_t)n; return; }
+    if (i == nitems) {
+        first[i] = (uint32_t)n;
+        return;
+    }
     uint64_t lo = 0, hi = n;
     while (lo < hi) {
         const uint64_t mid = (lo + hi) >> 1;
@@ -277,78 +286,37 @@ void launch_key_bounds(const uint64_t* keys, uint64_t n, const uint64_t* base, u
     PTC_CHECK_LAUNCH();
 }
 
-// local[j] = global[j] - first[item of element j] (element j of the concatenated side)
-__global__ void localize_kernel(const uint32_t* __restrict__ global, uint64_t n, const uint64_t* __restrict__ nnz_off,
+// local[j] = global[j] - first[item of element j]
+__global__ void localize_kernel(const uint32_t* __restrict__ global, uint64_t n, const uint64_t* __restrict__ off,
                                 uint32_t nitems, const uint32_t* __restrict__ first, uint32_t* __restrict__ local) {
     const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j < n) local[j] = global[j] - first[item_of(nnz_off, nitems, j)];
+    if (j < n) local[j] = global[j] - first[item_of(off, nitems, j)];
 }
 
-void launch_localize(const uint32_t* global, uint64_t n, const uint64_t* nnz_off, uint32_t nitems,
-                     const uint32_t* first, uint32_t* local, cudaStream_t st) {
+void launch_localize(const uint32_t* global, uint64_t n, const uint64_t* off, uint32_t nitems, const uint32_t* first,
+                     uint32_t* local, cudaStream_t st) {
     if (n == 0) return;
-    localize_kernel<<<ceil_div_u32(n, 256), 256, 0, st>>>(global, n, nnz_off, nitems, first, local);
+    localize_kernel<<<ceil_div_u32(n, 256), 256, 0, st>>>(global, n, off, nitems, first, local);
     count_launch();
     PTC_CHECK_LAUNCH();
 }
 
-// row_colbase[r] = col_first[item of row r], the item found from the row's first global row in
-// row_first (rows of item i are [row_first[i], row_first[i + 1]))
-__global__ void row_colbase_kernel(uint64_t nrows, const uint32_t* __restrict__ row_first,
-                                   const uint32_t* __restrict__ col_first, uint32_t nitems,
-                                   uint32_t* __restrict__ row_colbase) {
+// row_item[r] = the item whose rows [first[i], first[i + 1]) hold r
+__global__ void row_item_kernel(uint64_t nrows, const uint32_t* __restrict__ first, uint32_t nitems,
+                                uint32_t* __restrict__ row_item) {
     const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= nrows) return;
     uint32_t lo = 0, hi = nitems;
     while (hi - lo > 1) {
         const uint32_t mid = (lo + hi) >> 1;
-        if (row_first[mid] <= r) lo = mid; else hi = mid;
+        if (first[mid] <= r) lo = mid; else hi = mid;
     }
-    row_colbase[r] = col_first[lo];
+    row_item[r] = lo;
 }
 
-void launch_row_colbase(uint64_t nrows, const uint32_t* row_first, const uint32_t* col_first, uint32_t nitems,
-                        uint32_t* row_colbase, cudaStream_t st) {
+void launch_row_item(uint64_t nrows, const uint32_t* first, uint32_t nitems, uint32_t* row_item, cudaStream_t st) {
     if (nrows == 0) return;
-    row_colbase_kernel<<<ceil_div_u32(nrows, 256), 256, 0, st>>>(nrows, row_first, col_first, nitems, row_colbase);
-    count_launch();
-    PTC_CHECK_LAUNCH();
-}
-
-// Batch output: entries of item i are [ent[i], ent[i+1]) of the combined output, whose index
-// tuples are padded to fa_w + fb_w; copy them to the item's compact tuples at dst_off[i].
-__global__ void repack_kernel(const uint32_t* __restrict__ src, uint64_t total, const uint64_t* __restrict__ ent,
-                              uint32_t nitems, const ItemSpec* __restrict__ specs, uint32_t fa_w, uint32_t fb_w,
-                              const uint64_t* __restrict__ dst_off, uint32_t* __restrict__ dst) {
-    const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= total) return;
-    const uint32_t it = item_of(ent, nitems, e);
-    const uint32_t c = specs[it].c;
-    const uint32_t fa = specs[it].side[0].order - c, fb = specs[it].side[1].order - c;
-    const uint32_t* s = src + e * (fa_w + fb_w);
-    uint32_t* d = dst + dst_off[it] + (e - ent[it]) * (fa + fb);
-    for (uint32_t m = 0; m < fa; ++m) d[m] = s[m];
-    for (uint32_t m = 0; m < fb; ++m) d[fa + m] = s[fa_w + m];
-}
-
-void launch_repack(const uint32_t* src, uint64_t total, const uint64_t* ent, uint32_t nitems, const ItemSpec* specs,
-                   uint32_t fa_w, uint32_t fb_w, const uint64_t* dst_off, uint32_t* dst, cudaStream_t st) {
-    if (total == 0) return;
-    repack_kernel<<<ceil_div_u32(total, 256), 256, 0, st>>>(src, total, ent, nitems, specs, fa_w, fb_w, dst_off, dst);
-    count_launch();
-    PTC_CHECK_LAUNCH();
-}
-
-// ent[i] = row_off[row_first[i]]
-__global__ void item_entries_kernel(const uint64_t* __restrict__ row_off, const uint32_t* __restrict__ row_first,
-                                    uint32_t nitems, uint64_t* __restrict__ ent) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i <= nitems) ent[i] = row_off[row_first[i]];
-}
-
-void launch_item_entries(const uint64_t* row_off, const uint32_t* row_first, uint32_t nitems, uint64_t* ent,
-                         cudaStream_t st) {
-    item_entries_kernel<<<ceil_div_u32((uint64_t)nitems + 1, 128), 128, 0, st>>>(row_off, row_first, nitems, ent);
+    row_item_kernel<<<ceil_div_u32(nrows, 256), 256, 0, st>>>(nrows, first, nitems, row_item);
     count_launch();
     PTC_CHECK_LAUNCH();
 }

@@ -21,12 +21,13 @@ void launch_panel_offsets(const uint32_t* b_col, const uint32_t* b_fib, const ui
 
 // ---- batches ----
 
-// One side (A = 0, B = 1) of a batch item: where its nonzeros and indices start in the
-// concatenated arrays, its modes (contracted first), the strides that linearize them (contracted
-// key, then free key) and the base of its free-key range.
+// One side (A = 0, B = 1) of a batch item, as the device reads it: the item's COO arrays, its modes
+// (contracted first, then free in output order), their sizes, the strides that linearize them
+// (contracted key, then free key) and the base of its free-key range.
 struct ItemSide {
-    uint64_t idx_off;  // first u32 of the item's indices
-    uint64_t fbase;    // free keys of this item are fbase + [0, free key space)
+    const uint32_t* idx;  // [nnz * order], device memory
+    const double* vals;   // [nnz], device memory
+    uint64_t fbase;       // free keys of this item are fbase + [0, free key space)
     uint32_t order;
     uint32_t pad;
     uint32_t mode[kMaxOrder];
@@ -41,20 +42,15 @@ struct ItemSpec {
     ItemSide side[2];
 };
 
-void launch_pack_items(const uint32_t* idx, uint64_t nnz, const ItemSpec* specs, const uint64_t* nnz_off,
-                       uint32_t nitems, int side, uint64_t* ckey, uint64_t* fkey, uint32_t* err, cudaStream_t st);
-void launch_item_tuples(const uint32_t* idx, const uint32_t* run_start, const uint32_t* perm, uint64_t nruns,
-                        const ItemSpec* specs, const uint64_t* nnz_off, uint32_t nitems, int side, uint32_t width,
-                        uint32_t* tuple, cudaStream_t st);
+void launch_pack_items(const ItemSpec* specs, const uint64_t* off, uint32_t nitems, int side, uint64_t nnz,
+                       uint64_t* ckey, uint64_t* fkey, double* vals, uint32_t* err, cudaStream_t st);
+void launch_item_tuples(const uint32_t* run_start, const uint32_t* perm, uint64_t nruns, const ItemSpec* specs,
+                        const uint64_t* off, uint32_t nitems, int side, uint32_t width, uint32_t* tuple,
+                        cudaStream_t st);
 void launch_key_bounds(const uint64_t* keys, uint64_t n, const uint64_t* base, uint32_t nitems, uint32_t* first,
                        cudaStream_t st);
-void launch_localize(const uint32_t* global, uint64_t n, const uint64_t* nnz_off, uint32_t nitems,
-                     const uint32_t* first, uint32_t* local, cudaStream_t st);
-void launch_row_colbase(uint64_t nrows, const uint32_t* row_first, const uint32_t* col_first, uint32_t nitems,
-                        uint32_t* row_colbase, cudaStream_t st);
-void launch_repack(const uint32_t* src, uint64_t total, const uint64_t* ent, uint32_t nitems, const ItemSpec* specs,
-                   uint32_t fa_w, uint32_t fb_w, const uint64_t* dst_off, uint32_t* dst, cudaStream_t st);
-void launch_item_entries(const uint64_t* row_off, const uint32_t* row_first, uint32_t nitems, uint64_t* ent,
-                         cudaStream_t st);
+void launch_localize(const uint32_t* global, uint64_t n, const uint64_t* off, uint32_t nitems, const uint32_t* first,
+                     uint32_t* local, cudaStream_t st);
+void launch_row_item(uint64_t nrows, const uint32_t* first, uint32_t nitems, uint32_t* row_item, cudaStream_t st);
 
 }  // namespace ptc

@@ -5,6 +5,7 @@
 // the row grouping of A (buildHashTable(A_copy)), reorder_tensor (fksCuckooTC.hpp:31-77), the
 // symbolic pass (:94-154) and the numeric pass (:180-357).
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -14,6 +15,7 @@
 #include <dlfcn.h>
 #include <sys/mman.h>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "partc.h"
@@ -81,7 +83,7 @@ void validate_modes(const uint32_t* modes, uint32_t order, const char* name) {
 }
 
 struct Events {
-    static constexpr int kN = 8;
+    static constexpr int kN = 10;
     cudaEvent_t ev[kN] = {};
     explicit Events() {
         for (auto& e : ev) PTC_CUDA(cudaEventCreate(&e));
@@ -97,7 +99,7 @@ struct Events {
     }
 };
 
-enum { EV_START = 0, EV_H2D, EV_BSIDE, EV_ASIDE, EV_SYM, EV_NUM, EV_D2H };
+enum { EV_START = 0, EV_H2D, EV_BSIDE, EV_ASIDE, EV_SYM, EV_NUM, EV_D2H, EV_WAVE0, EV_WAVE1 };
 
 cudaStream_t default_stream_for_thread(int device) {
     thread_local int dev = -1;
@@ -150,6 +152,7 @@ struct Ranked {
     uint32_t* rank_of = nullptr;    // [n] rank of original element i
     uint32_t* run_of = nullptr;     // [n] rank of the i-th smallest
     uint32_t* run_start = nullptr;  // [nruns + 1] in sorted order
+    uint64_t* run_key = nullptr;    // [nruns] the distinct keys, increasing
     uint64_t nruns = 0;
 };
 
@@ -163,7 +166,8 @@ Ranked rank_keys(const uint64_t* keys, uint64_t n, uint64_t space, Arena& ar) {
     radix_sort_pairs(k, r.perm, n, 0, bits_for_space(space), ar);
     r.run_of = ar.alloc<uint32_t>(n);
     r.run_start = ar.alloc<uint32_t>(n + 1);
-    r.nruns = runs_of_sorted(k, n, r.run_of, r.run_start, nullptr, ar);
+    r.run_key = ar.alloc<uint64_t>(std::max<uint64_t>(n, 1));
+    r.nruns = runs_of_sorted(k, n, r.run_of, r.run_start, r.run_key, ar);
     r.rank_of = ar.alloc<uint32_t>(n);
     launch_scatter_u32(r.run_of, r.perm, n, r.rank_of, st);
     return r;
@@ -197,9 +201,58 @@ DeviceCoo to_device(const ptc_coo* t, Arena& ar) {
     return d;
 }
 
+// B entries grouped into fibers: sorted by (contracted key, column) with input order kept among
+// equal keys (reorder_tensor, fksCuckooTC.hpp:31-77), every fiber contiguous and ordered by column.
+struct Fibers {
+    uint64_t n = 0;
+    uint32_t* start = nullptr;  // [n + 1]
+    uint64_t* key = nullptr;    // [n] contracted key of each fiber
+    uint32_t* of = nullptr;     // [nb] fiber of each sorted entry
+    uint32_t* col = nullptr;    // [nb] column id of each sorted entry
+    double* val = nullptr;      // [nb]
+};
+
+// col_rank[j] = rank of entry j's free key among the ncols distinct ones; col_id (default
+// col_rank) is the column id stored for it.
+Fibers group_fibers(const uint64_t* ckey, const uint32_t* col_rank, uint64_t ncols, uint64_t nb, int cbits,
+                    const double* vals, Arena& ar, const uint32_t* col_id = nullptr) {
+    cudaStream_t st = ar.stream();
+    uint32_t* fperm = ar.alloc<uint32_t>(nb);
+    launch_iota(fperm, nb, st);
+    const int colbits = bits_for_space(std::max<uint64_t>(ncols, 1));
+    if (cbits + colbits <= 64) {
+        uint64_t* comp = ar.alloc<uint64_t>(nb);
+        launch_composite(ckey, col_rank, ncols, nb, comp, st);
+        radix_sort_pairs(comp, fperm, nb, 0, cbits + colbits, ar);
+    } else {
+        uint64_t* k = ar.alloc<uint64_t>(nb);
+        launch_composite(ckey, col_rank, 0, nb, k, st);  // 0 * ckey + col = col
+        radix_sort_pairs(k, fperm, nb, 0, colbits, ar);
+        launch_gather<uint64_t>(ckey, fperm, nb, k, st);
+        radix_sort_pairs(k, fperm, nb, 0, cbits, ar);
+    }
+    uint64_t* ckey_sorted = ar.alloc<uint64_t>(nb);
+    launch_gather<uint64_t>(ckey, fperm, nb, ckey_sorted, st);
+    Fibers f;
+    f.of = ar.alloc<uint32_t>(nb);
+    f.start = ar.alloc<uint32_t>(nb + 1);
+    f.key = ar.alloc<uint64_t>(std::max<uint64_t>(nb, 1));
+    f.n = runs_of_sorted(ckey_sorted, nb, f.of, f.start, f.key, ar);
+    f.col = ar.alloc<uint32_t>(nb);
+    f.val = ar.alloc<double>(nb);
+    launch_gather<uint32_t>(col_id ? col_id : col_rank, fperm, nb, f.col, st);
+    launch_gather<double>(vals, fperm, nb, f.val, st);
+    return f;
+}
+
 // Device -> pageable host copy of a large result: chunks go by DMA into two pinned staging
 // buffers while host threads copy the previous chunk out (and fault in the destination pages)
 // in parallel.  A plain cudaMemcpy into fresh pageable memory runs at a small fraction of this.
+struct HostSeg {
+    const void* src;
+    size_t bytes;
+};
+
 class HostCopier {
   public:
     static constexpr size_t kStage = 128ull << 20;
@@ -220,6 +273,43 @@ class HostCopier {
             parallel_memcpy(static_cast<char*>(dst) + off, static_cast<const char*>(stage_[c & 1]), n);
         }
     }
+    // Pageable host segments -> one contiguous device buffer, staged the same way.
+    void gather_to_device(void* dst, const std::vector<HostSeg>& segs, cudaStream_t st) {
+        size_t total = 0;
+        for (const HostSeg& g : segs) total += g.bytes;
+        if (total == 0) return;
+        ensure();
+        struct Piece {
+            const char* src;
+            size_t off, n;
+        };
+        size_t seg = 0, seg_off = 0, done = 0;
+        for (size_t c = 0; done < total; ++c) {
+            const size_t n = std::min(kStage, total - done);
+            std::vector<Piece> pieces;
+            for (size_t filled = 0; filled < n;) {
+                const size_t take = std::min(segs[seg].bytes - seg_off, n - filled);
+                for (size_t o = 0; o < take; o += kBlock)  // at most 1 MiB per piece
+                    pieces.push_back({static_cast<const char*>(segs[seg].src) + seg_off + o, filled + o,
+                                      std::min(kBlock, take - o)});
+                filled += take;
+                seg_off += take;
+                if (seg_off == segs[seg].bytes) {
+                    ++seg;
+                    seg_off = 0;
+                }
+            }
+            char* stage = static_cast<char*>(stage_[c & 1]);
+            PTC_CUDA(cudaEventSynchronize(ev_[c & 1]));  // its previous copy has left the buffer
+            const int64_t np = (int64_t)pieces.size();
+#pragma omp parallel for schedule(dynamic, 4)
+            for (int64_t i = 0; i < np; ++i) std::memcpy(stage + pieces[i].off, pieces[i].src, pieces[i].n);
+            PTC_CUDA(cudaMemcpyAsync(static_cast<char*>(dst) + done, stage, n, cudaMemcpyHostToDevice, st));
+            PTC_CUDA(cudaEventRecord(ev_[c & 1], st));
+            done += n;
+        }
+        for (int i = 0; i < 2; ++i) PTC_CUDA(cudaEventSynchronize(ev_[i]));
+    }
     ~HostCopier() {
         for (int i = 0; i < 2; ++i) {
             if (stage_[i]) cudaFreeHost(stage_[i]);
@@ -235,8 +325,8 @@ class HostCopier {
             PTC_CUDA(cudaEventCreateWithFlags(&ev_[i], cudaEventDisableTiming));
         }
     }
+    static constexpr size_t kBlock = 1ull << 20;
     static void parallel_memcpy(char* dst, const char* src, size_t n) {
-        constexpr size_t kBlock = 1ull << 20;
         const int64_t nb = (int64_t)((n + kBlock - 1) / kBlock);
 #pragma omp parallel for schedule(static)
         for (int64_t b = 0; b < nb; ++b) {
@@ -297,7 +387,67 @@ const SizerHost* default_sizer() {
     return s ? &s->host : nullptr;
 }
 
-// Grow the claimable output to `need` entries, keeping the first `used`.
+ptc_options resolve_options(const ptc_options* opt_in) {
+    ptc_options opt;
+    ptc_options_init(&opt);
+    if (opt_in) {
+        PTC_REQUIRE(opt_in->struct_size >= offsetof(ptc_options, reserved), PTC_ERR_INVALID_ARGUMENT,
+                    "ptc_options.struct_size too small (call ptc_options_init)");
+        std::memcpy(&opt, opt_in, std::min<size_t>(opt_in->struct_size, sizeof(opt)));
+    }
+    PTC_REQUIRE(opt.output_location == PTC_HOST || opt.output_location == PTC_DEVICE, PTC_ERR_INVALID_ARGUMENT,
+                "bad output_location");
+    PTC_REQUIRE(opt.panel_width == 0 || (opt.panel_width >= 32 && opt.panel_width <= 4096 &&
+                                         (opt.panel_width & (opt.panel_width - 1)) == 0),
+                PTC_ERR_INVALID_ARGUMENT, "panel_width must be 0 or a power of two in [32, 4096]");
+    PTC_REQUIRE(opt.path == PTC_PATH_TWO_PHASE || opt.path == PTC_PATH_LEARNED, PTC_ERR_INVALID_ARGUMENT,
+                "bad path");
+    return opt;
+}
+
+// The argument checks of one contraction (`where` prefixes the messages).
+void validate_pair(const ptc_coo* A, const ptc_coo* B, uint32_t c, const uint32_t* a_modes, const uint32_t* b_modes,
+                   const std::string& where) {
+    validate_coo(A, (where + "A").c_str());
+    validate_coo(B, (where + "B").c_str());
+    PTC_REQUIRE(c >= 1 && c <= A->order && c <= B->order, PTC_ERR_INVALID_ARGUMENT,
+                where + "need 1 <= c <= order of each tensor");
+    validate_modes(a_modes, A->order, (where + "a_modes").c_str());
+    validate_modes(b_modes, B->order, (where + "b_modes").c_str());
+    for (uint32_t j = 0; j < c; ++j)
+        PTC_REQUIRE(A->dims[a_modes[j]] == B->dims[b_modes[j]], PTC_ERR_INVALID_ARGUMENT,
+                    where + "paired contracted modes have different sizes");
+    PTC_REQUIRE(A->order - c + B->order - c >= 1, PTC_ERR_EMPTY_CONTRACTION,
+                where + "tensor contraction not possible (no free modes)");
+}
+
+struct DeviceSetup {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int num_sms = 0;
+};
+
+DeviceSetup setup_device(const ptc_options& opt) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        throw Error{PTC_ERR_NO_DEVICE, "no usable CUDA device"};
+    }
+    DeviceSetup d;
+    d.device = opt.device;
+    if (d.device < 0) PTC_CUDA(cudaGetDevice(&d.device));
+    PTC_REQUIRE(d.device < ndev, PTC_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+    PTC_CUDA(cudaSetDevice(d.device));
+    int major = 0;
+    PTC_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, d.device));
+    if (major != 10) throw Error{PTC_ERR_NO_DEVICE, "this library is built for sm_100a (B200) only"};
+    keep_pool_memory(d.device);
+    d.stream = opt.stream ? static_cast<cudaStream_t>(opt.stream) : default_stream_for_thread(d.device);
+    d.num_sms = device_sm_count(d.device);
+    return d;
+}
+
+// Grow the claimable output of a single contraction to `need` entries, keeping the first `used`.
 void grow_output(OutputView& ov, uint32_t od, uint64_t used, uint64_t need, cudaStream_t st) {
     uint32_t* idx = nullptr;
     double* val = nullptr;
@@ -312,10 +462,11 @@ void grow_output(OutputView& ov, uint32_t od, uint64_t used, uint64_t need, cuda
     ov.capacity = need;
 }
 
-// Learned path, after the first numeric pass: parts whose accumulator or output claim did not
-// fit their prediction wrote nothing and are listed in ov.fail_list.  Their rows get the exact
-// symbolic pass, each failed part is re-split exactly, and the new parts run (their sizes are
-// exact, so they cannot fail again).  Returns the output nnz.
+// Learned path of a single contraction, after the first numeric pass: parts whose accumulator
+// overflowed or whose claim did not fit wrote nothing and are listed in ov.fail_list.  Their rows
+// get the exact symbolic pass, each failed part is re-split exactly, and the new parts claim
+// after the entries already written (their sizes are exact, so they cannot fail again).  Returns
+// the output nnz.
 uint64_t learned_reruns(const Operands& op, const PartItem* parts, uint32_t n_parts, const uint32_t* big_rows,
                         uint32_t n_big, const float* pred, const SplitRule& rule, OutputView& ov,
                         uint32_t* work_counter, uint32_t* err, int num_sms, uint64_t nrows, Arena& ar,
@@ -337,8 +488,7 @@ uint64_t learned_reruns(const Operands& op, const PartItem* parts, uint32_t n_pa
         PTC_CUDA(cudaMemcpyAsync(hf.data(), failed, nfail * sizeof(PartItem), cudaMemcpyDeviceToHost, st));
         PTC_CUDA(cudaStreamSynchronize(st));
         std::vector<uint32_t> hrows, hridx(nfail);
-        std::vector<int64_t> seen;  // small: failed parts are few
-        for (uint32_t i = 0; i < nfail; ++i) {
+        for (uint32_t i = 0; i < nfail; ++i) {  // failed parts are few
             uint32_t r = 0;
             while (r < hrows.size() && hrows[r] != hf[i].row) ++r;
             if (r == hrows.size()) hrows.push_back(hf[i].row);
@@ -361,9 +511,12 @@ uint64_t learned_reruns(const Operands& op, const PartItem* parts, uint32_t n_pa
         const uint32_t nnew = read_scalar(np + nfail, st);
         uint64_t* need = ar.alloc<uint64_t>(1);
         launch_sum_u32(tot, nfail, need, st);
-        const uint64_t used = read_scalar(ov.cursor, st);
+        // the successful claims fill [0, cursor - overshoot); later claims start there
+        const uint64_t used = read_scalar(ov.cursor, st) - read_scalar(ov.overshoot, st);
         const uint64_t want = used + read_scalar(need, st);
         if (want > ov.capacity) grow_output(ov, op.fa + op.fb, used, want + 1024, st);
+        PTC_CUDA(cudaMemcpyAsync(ov.cursor, &used, sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+        PTC_CUDA(cudaMemsetAsync(ov.overshoot, 0, sizeof(uint64_t), st));
         PartItem* fresh = ar.alloc<PartItem>(nnew);
         launch_fill_parts_range(failed, dridx, nfail, cnt, P, rule, np, fresh, st);
         ov.fail_list = ar.alloc<uint32_t>(std::max<uint32_t>(nnew, 1));
@@ -377,7 +530,7 @@ uint64_t learned_reruns(const Operands& op, const PartItem* parts, uint32_t n_pa
     double* esum = ar.alloc<double>(1);
     launch_log2_error(big_rows, n_big, pred, row_actual, esum, st);
     stats.sizer_mean_abs_log2_err = n_big ? read_scalar(esum, st) / n_big : 0.0;
-    return read_scalar(ov.cursor, st);
+    return read_scalar(ov.cursor, st) - read_scalar(ov.overshoot, st);
 }
 
 // Training samples of the learned sizer, gathered instead of running the numeric pass.
@@ -386,64 +539,263 @@ struct Collect {
     std::vector<float> t;  // n
 };
 
-void contract_impl(const ptc_coo* A, const ptc_coo* Bin, uint32_t c, const uint32_t* a_modes,
-                   const uint32_t* b_modes_in, const ptc_options* opt_in, ptc_tensor* out, ptc_stats* stats_out,
-                   Collect* collect = nullptr) {
-    ptc_options opt;
-    ptc_options_init(&opt);
-    if (opt_in) {
-        PTC_REQUIRE(opt_in->struct_size >= offsetof(ptc_options, reserved), PTC_ERR_INVALID_ARGUMENT,
-                    "ptc_options.struct_size too small (call ptc_options_init)");
-        std::memcpy(&opt, opt_in, std::min<size_t>(opt_in->struct_size, sizeof(opt)));
-    }
-    PTC_REQUIRE(out != nullptr, PTC_ERR_INVALID_ARGUMENT, "out is null");
-    std::memset(out, 0, sizeof(*out));
-    ptc_stats stats;
-    std::memset(&stats, 0, sizeof(stats));
-    g_launches = 0;
+// What the build phase hands to planning: the grouped operands and, for a batch, where each
+// item's rows and columns lie.
+struct Front {
+    Operands op;
+    const uint32_t* b_fib = nullptr;  // fiber of each sorted B entry
+    const uint32_t* a_row = nullptr;  // row of each sorted A element
+    bool batch = false;
+    uint32_t nitems = 1;
+    uint32_t* row_first = nullptr;        // device [nitems + 1]: item i owns rows [row_first[i], row_first[i+1])
+    std::vector<uint32_t> h_row_first;    // host copy
+    std::vector<uint32_t> colbase;        // first global column of each item
+    std::vector<uint32_t> item_fa, item_fb;
+    ItemOut* item_out = nullptr;          // device [nitems], filled per wave
+};
 
-    const bool self = (Bin == nullptr);
-    const ptc_coo* B = self ? A : Bin;
-    const uint32_t* b_modes = self ? a_modes : b_modes_in;
-    validate_coo(A, "A");
-    validate_coo(B, "B");
-    PTC_REQUIRE(c >= 1 && c <= A->order && c <= B->order, PTC_ERR_INVALID_ARGUMENT,
-                "need 1 <= c <= order of each tensor");
-    validate_modes(a_modes, A->order, "a_modes");
-    validate_modes(b_modes, B->order, "b_modes");
-    for (uint32_t j = 0; j < c; ++j)
-        PTC_REQUIRE(A->dims[a_modes[j]] == B->dims[b_modes[j]], PTC_ERR_INVALID_ARGUMENT,
-                    "paired contracted modes have different sizes");
+// Tuning knobs (the autotuner's search space), resolved from the options.
+struct Knobs {
+    uint32_t small_max;  // products of the largest row on the one-warp accumulator
+    uint32_t esc_avg;    // sort-based rows: fewer products per A nonzero than this on average
+    double max_load;     // cuckoo table load factor
+};
+
+Knobs knobs_of(const ptc_options& opt) {
+    Knobs k;
+    k.small_max = opt.small_max_products ? std::min(opt.small_max_products, small_row_max_flops())
+                                         : small_row_max_flops();
+    k.esc_avg = opt.sort_max_avg_products ? opt.sort_max_avg_products : kEscMaxAvgProducts;
+    k.max_load = opt.hash_load_pct ? std::min(std::max(opt.hash_load_pct, 10u), 90u) / 100.0 : 0.75;
+    return k;
+}
+
+// The row classes, the sizes and the work items of one contraction or batch.
+struct Plan {
+    bool learned = false;
+    uint64_t flops = 0;
+    uint32_t W = 0, log2w = 0, P = 1;
+    uint64_t* row_flops = nullptr;
+    uint32_t n_small = 0, n_big = 0, n_esc = 0;
+    uint32_t* small_rows = nullptr;  // in row order
+    uint32_t* big_rows = nullptr;    // largest first
+    uint32_t* esc_rows = nullptr;    // in row order
+    uint32_t* small_pos = nullptr;   // [nrows + 1] small rows before each row
+    uint32_t* esc_pos = nullptr;     // [nrows + 1] sort-based rows before each row
+    // sort-based rows: runs of equal (row, column) in the sorted products
+    uint64_t esc_runs = 0;
+    uint32_t esc_colbits = 0;
+    uint64_t* esc_run_key = nullptr;
+    uint32_t* esc_run_start = nullptr;
+    uint32_t* esc_first = nullptr;  // [n_esc + 1] first run of each sort-based row
+    double* esc_sorted = nullptr;   // products in run order
+    // sizes: exact offsets of the small and sort-based rows (and, on the two-phase path, of every
+    // row); the learned path's large rows claim instead, within claim_off's budgets
+    uint64_t* row_off = nullptr;
+    uint64_t* claim_off = nullptr;
+    uint64_t exact_nnz = 0, claim_total = 0;
+    float* pred = nullptr;
+    SplitRule rule{};
+    PartItem* parts = nullptr;
+    uint32_t n_parts = 0;
+    uint32_t* work_counter = nullptr;
+    bool collected = false;
+};
+
+Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect* collect, int num_sms, Arena& ar,
+               ptc_stats& stats) {
+    cudaStream_t st = ar.stream();
+    Operands& op = F.op;
+    const uint64_t na = op.na, nb = op.nb, nrows = op.nrows, ncols = op.ncols, nfib = op.nfib;
+    const Knobs kn = knobs_of(opt);
+    Plan pl;
+    pl.learned = sizer != nullptr;
+
+    // flops per row
+    uint64_t* alen = ar.alloc<uint64_t>(na + 1);
+    launch_fiber_len(op.a_fib, op.fib_start, na, alen, st);
+    exclusive_scan<uint64_t>(alen, alen, na, ar);
+    pl.row_flops = ar.alloc<uint64_t>(std::max<uint64_t>(nrows, 1));
+    launch_row_flops(alen, op.row_start, nrows, pl.row_flops, st);
+    pl.flops = read_scalar(alen + na, st);
+    stats.mult_adds = pl.flops;
+    stats.nrows = nrows;
+    stats.nfibers = nfib;
+    if (pl.flops == 0) return pl;
+
+    // fine column panels: B fibers are split at multiples of W so a row can be cut into parts
+    // that each fit one shared-memory table (W <= table capacity, so a part always fits).  The
+    // per-fiber panel table is kept within 1 GiB (wider panels, else binary searches in the fiber).
+    PTC_REQUIRE(ncols <= sym_bitmap_max_cols(), PTC_ERR_INVALID_ARGUMENT,
+                "more than 1.5M distinct B free keys in one contraction is not supported yet");
+    auto table_bytes = [&](uint32_t w) { return nfib * ((ncols + w - 1) / w + 1) * 4; };
+    uint32_t W = opt.panel_width;
+    if (W == 0) {
+        W = 32;
+        while (W < 2048 && (uint64_t)W * 16 < ncols) W <<= 1;
+        uint32_t w2 = W;
+        while (w2 < 4096 && table_bytes(w2) > (1ull << 30)) w2 <<= 1;
+        if (table_bytes(w2) <= (1ull << 30)) W = w2;
+    }
+    PTC_REQUIRE(W <= hash_part_capacity(), PTC_ERR_INVALID_ARGUMENT, "panel_width larger than a hash part");
+    pl.W = W;
+    pl.log2w = floor_log2(W);
+    pl.P = (uint32_t)std::max<uint64_t>(1, (ncols + W - 1) / W);
+    const uint32_t P = pl.P;
+    stats.panel_width = W;
+    uint32_t* panel_off = nullptr;
+    if (P > 1 && table_bytes(W) <= (1ull << 30)) {
+        panel_off = ar.alloc<uint32_t>(nfib * (uint64_t)(P + 1));
+        launch_panel_offsets(op.b_col, F.b_fib, op.fib_start, nb, P, pl.log2w, panel_off, st);
+    }
+    op.panel_off = panel_off;
+    op.npanels = P;
+    op.panel_log2 = pl.log2w;
+
+    // row classes and work lists (largest rows first)
+    uint32_t* small_flag = ar.alloc<uint32_t>(nrows + 1);
+    uint32_t* big_flag = ar.alloc<uint32_t>(nrows + 1);
+    uint32_t* esc_flag = ar.alloc<uint32_t>(nrows + 1);
+    launch_classify_rows(pl.row_flops, op.row_start, nrows, kn.small_max, kn.esc_avg, small_flag, big_flag, esc_flag,
+                         st);
+    pl.esc_pos = ar.alloc<uint32_t>(nrows + 1);
+    exclusive_scan<uint32_t>(esc_flag, pl.esc_pos, nrows, ar);
+    pl.n_esc = read_scalar(pl.esc_pos + nrows, st);
+    pl.esc_rows = ar.alloc<uint32_t>(pl.n_esc);
+    launch_compact_indices(esc_flag, pl.esc_pos, nrows, pl.esc_rows, st);
+    uint64_t* esc_off = ar.alloc<uint64_t>((uint64_t)pl.n_esc + 1);
+    uint64_t f_esc = 0;
+    const int colbits = bits_for_space(std::max<uint64_t>(ncols, 1));
+    if (pl.n_esc > 0) {
+        launch_esc_len(pl.esc_rows, pl.n_esc, pl.row_flops, esc_off, st);
+        exclusive_scan<uint64_t>(esc_off, esc_off, pl.n_esc, ar);
+        f_esc = read_scalar(esc_off + pl.n_esc, st);
+        if (f_esc > kEscMaxProducts || bits_for_space((uint64_t)pl.n_esc) + colbits > 64) {
+            // too large for the sort buffers: hash path
+            launch_merge_flags(big_flag, esc_flag, nrows, st);
+            PTC_CUDA(cudaMemsetAsync(pl.esc_pos, 0, (nrows + 1) * sizeof(uint32_t), st));
+            pl.n_esc = 0;
+            f_esc = 0;
+        }
+    }
+    pl.small_pos = ar.alloc<uint32_t>(nrows + 1);
+    uint32_t* big_pos = ar.alloc<uint32_t>(nrows + 1);
+    exclusive_scan<uint32_t>(small_flag, pl.small_pos, nrows, ar);
+    exclusive_scan<uint32_t>(big_flag, big_pos, nrows, ar);
+    pl.n_small = read_scalar(pl.small_pos + nrows, st);
+    pl.n_big = read_scalar(big_pos + nrows, st);
+    pl.small_rows = ar.alloc<uint32_t>(pl.n_small);
+    pl.big_rows = ar.alloc<uint32_t>(pl.n_big);
+    launch_compact_indices(small_flag, pl.small_pos, nrows, pl.small_rows, st);
+    launch_compact_indices(big_flag, big_pos, nrows, pl.big_rows, st);
+    const uint32_t n_small = pl.n_small, n_big = pl.n_big, n_esc = pl.n_esc;
+    if (n_big > 1) {
+        uint64_t* wkey = ar.alloc<uint64_t>(n_big);
+        launch_work_keys(pl.big_rows, n_big, pl.row_flops, wkey, st);
+        radix_sort_pairs(wkey, pl.big_rows, n_big, 0, 40, ar);
+    }
+    stats.rows_small = n_small;
+    stats.rows_hash = n_big;
+    stats.rows_long = n_esc;
+
+    pl.rule.cap = hash_part_capacity();
+    pl.rule.dense_panels = dense_part_columns() >> pl.log2w;
+    pl.rule.dense_min = W / kDenseMinFraction;
+    pl.rule.min_bits = hash_part_min_bits();
+
+    // symbolic: exact output nnz of the small rows (both paths) and of the large rows (per fine
+    // panel; two-phase path only -- the learned path predicts those)
+    uint64_t* row_d = ar.alloc<uint64_t>(nrows + 1);
+    PTC_CUDA(cudaMemsetAsync(row_d, 0, (nrows + 1) * sizeof(uint64_t), st));
+    uint32_t* panel_cnt = ar.alloc<uint32_t>((uint64_t)n_big * P);
+    pl.work_counter = ar.alloc<uint32_t>(1);
+    OutputView none;
+    launch_small_rows(false, op, pl.small_rows, n_small, row_d, nullptr, none, st);
+    if (!pl.learned) launch_sym_bitmap(op, pl.big_rows, n_big, panel_cnt, row_d, pl.work_counter, num_sms, st);
+    // sort-based rows: expand their products in stream order, sort stably by (row, column)
+    pl.esc_colbits = (uint32_t)colbits;
+    if (n_esc > 0) {
+        int32_t* esc_of = ar.alloc<int32_t>(nrows);
+        PTC_CUDA(cudaMemsetAsync(esc_of, 0xff, nrows * sizeof(int32_t), st));
+        launch_esc_index(pl.esc_rows, n_esc, esc_of, st);
+        uint64_t* esc_key = ar.alloc<uint64_t>(f_esc);
+        double* esc_val = ar.alloc<double>(f_esc);
+        uint32_t* esc_perm = ar.alloc<uint32_t>(f_esc);
+        launch_esc_expand(op, F.a_row, esc_of, alen, esc_off, pl.esc_colbits, esc_key, esc_val, esc_perm, st);
+        radix_sort_pairs(esc_key, esc_perm, f_esc, 0, pl.esc_colbits + bits_for_space((uint64_t)n_esc), ar);
+        pl.esc_run_start = ar.alloc<uint32_t>(f_esc + 1);
+        pl.esc_run_key = ar.alloc<uint64_t>(f_esc);
+        pl.esc_runs = runs_of_sorted(esc_key, f_esc, nullptr, pl.esc_run_start, pl.esc_run_key, ar);
+        pl.esc_first = ar.alloc<uint32_t>((uint64_t)n_esc + 1);
+        launch_esc_count(pl.esc_run_key, pl.esc_runs, pl.esc_colbits, pl.esc_rows, row_d, pl.esc_first, st);
+        const uint32_t total_runs = (uint32_t)pl.esc_runs;
+        PTC_CUDA(cudaMemcpyAsync(pl.esc_first + n_esc, &total_runs, sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        // the products in run order (the sort keys are no longer needed: their buffer takes them)
+        pl.esc_sorted = reinterpret_cast<double*>(esc_key);
+        launch_esc_gather(esc_perm, esc_val, f_esc, pl.esc_sorted, st);
+    }
+    pl.row_off = ar.alloc<uint64_t>(nrows + 1);
+    exclusive_scan<uint64_t>(row_d, pl.row_off, nrows, ar);
+    pl.exact_nnz = read_scalar(pl.row_off + nrows, st);
+
+    if (collect) {
+        // features of the rows the learned path sizes, and log2(1 + their exact output nnz)
+        float* gp = ar.alloc<float>((uint64_t)(P + 1) * kGridPoints);
+        launch_popularity_table(op.b_col, nb, ncols, P, pl.log2w, gp, ar);
+        float* fx = ar.alloc<float>((uint64_t)n_big * kSizerInputs);
+        float* ft = ar.alloc<float>(n_big);
+        launch_row_features(op, pl.big_rows, n_big, pl.row_flops, gp, fx, st);
+        launch_row_targets(pl.big_rows, n_big, row_d, ft, st);
+        collect->x.resize((uint64_t)n_big * kSizerInputs);
+        collect->t.resize(n_big);
+        PTC_CUDA(cudaMemcpyAsync(collect->x.data(), fx, collect->x.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+        PTC_CUDA(cudaMemcpyAsync(collect->t.data(), ft, collect->t.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+        PTC_CUDA(cudaStreamSynchronize(st));
+        pl.collected = true;
+        return pl;
+    }
+
+    if (pl.learned) {
+        pl.claim_off = ar.alloc<uint64_t>(nrows + 1);
+        PTC_CUDA(cudaMemsetAsync(pl.claim_off, 0, (nrows + 1) * sizeof(uint64_t), st));
+        if (n_big > 0) {
+            // sizer: per-row features -> predicted log2(1 + nnz) -> per-panel counts by column popularity
+            float* gp = ar.alloc<float>((uint64_t)(P + 1) * kGridPoints);
+            launch_popularity_table(op.b_col, nb, ncols, P, pl.log2w, gp, ar);
+            float* fx = ar.alloc<float>((uint64_t)n_big * kSizerInputs);
+            launch_row_features(op, pl.big_rows, n_big, pl.row_flops, gp, fx, st);
+            pl.pred = ar.alloc<float>(n_big);
+            sizer_predict_device(*sizer, fx, n_big, pl.pred, ar);
+            launch_predicted_panel_counts(pl.big_rows, n_big, pl.row_flops, pl.pred, gp, P, pl.log2w, ncols,
+                                          kSizerMargin, panel_cnt, st);
+            launch_claim_budgets(pl.big_rows, n_big, panel_cnt, P, pl.claim_off, st);
+        }
+        exclusive_scan<uint64_t>(pl.claim_off, pl.claim_off, nrows, ar);
+        pl.claim_total = read_scalar(pl.claim_off + nrows, st);
+    }
+
+    // split large rows into parts that fit a shared-memory table
+    uint32_t* nparts = ar.alloc<uint32_t>((uint64_t)n_big + 1);
+    launch_count_parts(panel_cnt, n_big, P, pl.rule, nparts, op.err, st);
+    exclusive_scan<uint32_t>(nparts, nparts, n_big, ar);
+    pl.n_parts = read_scalar(nparts + n_big, st);
+    PTC_REQUIRE(read_scalar(op.err, st) == 0, PTC_ERR_INTERNAL, "a fine panel exceeds the hash part capacity");
+    pl.parts = ar.alloc<PartItem>(pl.n_parts);
+    launch_fill_parts(pl.big_rows, panel_cnt, n_big, P, pl.rule, nparts, pl.learned ? nullptr : pl.row_off, pl.parts,
+                      st);
+    stats.hash_parts = pl.n_parts;
+    return pl;
+}
+
+// ---------------------------------------------------------------------------------------------
+// single contraction
+// ---------------------------------------------------------------------------------------------
+
+Front front_single(const ptc_coo* A, const ptc_coo* B, bool self, uint32_t c, const uint32_t* a_modes,
+                   const uint32_t* b_modes, const ptc_options& opt, const Knobs& kn, Arena& ar, Events& ev,
+                   ptc_stats& stats) {
+    cudaStream_t st = ar.stream();
     const uint32_t fa = A->order - c, fb = B->order - c;
-    PTC_REQUIRE(fa + fb >= 1, PTC_ERR_EMPTY_CONTRACTION, "tensor contraction not possible (no free modes)");
-    if (self) PTC_REQUIRE(A->nnz > 1, PTC_ERR_TOO_FEW_NONZEROS, "Tensor B has at most one nonzeros");
-    PTC_REQUIRE(opt.output_location == PTC_HOST || opt.output_location == PTC_DEVICE, PTC_ERR_INVALID_ARGUMENT,
-                "bad output_location");
-    PTC_REQUIRE(opt.panel_width == 0 || (opt.panel_width >= 32 && opt.panel_width <= 4096 &&
-                                         (opt.panel_width & (opt.panel_width - 1)) == 0),
-                PTC_ERR_INVALID_ARGUMENT, "panel_width must be 0 or a power of two in [32, 4096]");
-
-    // device
-    int ndev = 0;
-    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
-        cudaGetLastError();
-        throw Error{PTC_ERR_NO_DEVICE, "no usable CUDA device"};
-    }
-    int device = opt.device;
-    if (device < 0) PTC_CUDA(cudaGetDevice(&device));
-    PTC_REQUIRE(device < ndev, PTC_ERR_INVALID_ARGUMENT, "device ordinal out of range");
-    PTC_CUDA(cudaSetDevice(device));
-    int major = 0;
-    PTC_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
-    if (major != 10) throw Error{PTC_ERR_NO_DEVICE, "this library is built for sm_100a (B200) only"};
-    keep_pool_memory(device);
-    cudaStream_t st = opt.stream ? static_cast<cudaStream_t>(opt.stream) : default_stream_for_thread(device);
-    const int num_sms = device_sm_count(device);
-
-    Events ev;
-    Arena ar(st);
-    PTC_CUDA(cudaEventRecord(ev.ev[EV_START], st));
-
     // ---- inputs on the device ----
     DeviceCoo dA = to_device(A, ar);
     DeviceCoo dB = self ? dA : to_device(B, ar);
@@ -476,35 +828,9 @@ void contract_impl(const ptc_coo* A, const ptc_coo* Bin, uint32_t c, const uint3
     const uint64_t ncols = cols.nruns;
     uint32_t* col_tuple = ar.alloc<uint32_t>(ncols * std::max(fb, 1u));
     launch_tuples(dB.idx, dB.order, cols.run_start, cols.perm, ncols, b_free, col_tuple, st);
-
-    uint32_t* fperm = ar.alloc<uint32_t>(nb);
-    launch_iota(fperm, nb, st);
-    const int cbits = bits_for_space(b_con.space);
-    const int colbits = bits_for_space(std::max<uint64_t>(ncols, 1));
-    if (cbits + colbits <= 64) {
-        uint64_t* comp = ar.alloc<uint64_t>(nb);
-        launch_composite(b_ckey, cols.rank_of, ncols, nb, comp, st);
-        radix_sort_pairs(comp, fperm, nb, 0, cbits + colbits, ar);
-    } else {
-        uint64_t* k = ar.alloc<uint64_t>(nb);
-        launch_composite(b_ckey, cols.rank_of, 0, nb, k, st);  // 0 * ckey + col = col
-        radix_sort_pairs(k, fperm, nb, 0, colbits, ar);
-        launch_gather<uint64_t>(b_ckey, fperm, nb, k, st);
-        radix_sort_pairs(k, fperm, nb, 0, cbits, ar);
-    }
-    uint64_t* b_ckey_sorted = ar.alloc<uint64_t>(nb);
-    launch_gather<uint64_t>(b_ckey, fperm, nb, b_ckey_sorted, st);
-    uint32_t* b_fib = ar.alloc<uint32_t>(nb);
-    uint32_t* fib_start = ar.alloc<uint32_t>(nb + 1);
-    uint64_t* fib_key = ar.alloc<uint64_t>(nb);
-    const uint64_t nfib = runs_of_sorted(b_ckey_sorted, nb, b_fib, fib_start, fib_key, ar);
-    uint32_t* b_col = ar.alloc<uint32_t>(nb);
-    double* b_val = ar.alloc<double>(nb);
-    launch_gather<uint32_t>(cols.rank_of, fperm, nb, b_col, st);
-    launch_gather<double>(dB.vals, fperm, nb, b_val, st);
-
+    Fibers fib = group_fibers(b_ckey, cols.rank_of, ncols, nb, bits_for_space(b_con.space), dB.vals, ar);
     CuckooBuildInfo cinfo;
-    const CuckooTable table = cuckoo_build(fib_key, nfib, opt.hash_seed, 64, 0.75, 8, ar, &cinfo);
+    const CuckooTable table = cuckoo_build(fib.key, fib.n, opt.hash_seed, 64, kn.max_load, 8, ar, &cinfo);
     stats.hash_attempts = cinfo.attempts;
     PTC_CUDA(cudaEventRecord(ev.ev[EV_BSIDE], st));
 
@@ -519,7 +845,6 @@ void contract_impl(const ptc_coo* A, const ptc_coo* Bin, uint32_t c, const uint3
         row_tuple = ar.alloc<uint32_t>(rows.nruns * std::max(fa, 1u));
         launch_tuples(dA.idx, dA.order, rows.run_start, rows.perm, rows.nruns, a_free, row_tuple, st);
     }
-    const uint64_t nrows = rows.nruns;
     uint64_t* a_ckey_sorted = ar.alloc<uint64_t>(na);
     double* a_val = ar.alloc<double>(na);
     launch_gather<uint64_t>(a_ckey, rows.perm, na, a_ckey_sorted, st);
@@ -528,95 +853,50 @@ void contract_impl(const ptc_coo* A, const ptc_coo* Bin, uint32_t c, const uint3
     cuckoo_lookup(table, a_ckey_sorted, na, a_fib, ar);
     PTC_CUDA(cudaEventRecord(ev.ev[EV_ASIDE], st));
 
-    // ---- symbolic: flops per row, accumulator bins, exact output nnz per work item ----
-    uint64_t* alen = ar.alloc<uint64_t>(na + 1);
-    launch_fiber_len(a_fib, fib_start, na, alen, st);
-    exclusive_scan<uint64_t>(alen, alen, na, ar);
-    uint64_t* row_flops = ar.alloc<uint64_t>(nrows);
-    launch_row_flops(alen, rows.run_start, nrows, row_flops, st);
-    std::vector<uint64_t> h_flops(nrows);
-    PTC_CUDA(cudaMemcpyAsync(h_flops.data(), row_flops, nrows * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
-    PTC_CUDA(cudaStreamSynchronize(st));
-    uint64_t flops = 0;
-    for (uint64_t f : h_flops) flops += f;
-    stats.mult_adds = flops;
-    stats.nrows = nrows;
-    stats.ncols = ncols;
-    stats.nfibers = nfib;
-    PTC_REQUIRE(flops > 0, PTC_ERR_EMPTY_CONTRACTION, "tensor contraction not possible!! (no matching fibers)");
-
-    // fine column panels: B fibers are split at multiples of W so a row can be cut into parts
-    // that each fit one shared-memory table (W <= table capacity, so a part always fits)
-    PTC_REQUIRE(ncols <= sym_bitmap_max_cols(), PTC_ERR_INVALID_ARGUMENT,
-                "more than 1.5M distinct B free keys is not supported yet");
-    // default: panels of 2048 columns (finer for narrow column spaces), the split table within 1 GiB
-    uint32_t W = opt.panel_width;
-    if (W == 0) {
-        W = 32;
-        while (W < 2048 && (uint64_t)W * 16 < ncols) W <<= 1;
-        while (W < 4096 && nfib * ((ncols + W - 1) / W + 1) * 4 > (1ull << 30)) W <<= 1;
-    }
-    PTC_REQUIRE(W <= hash_part_capacity(), PTC_ERR_INVALID_ARGUMENT, "panel_width larger than a hash part");
-    const uint32_t log2w = floor_log2(W);
-    const uint32_t P = (uint32_t)std::max<uint64_t>(1, (ncols + W - 1) / W);
-    stats.panel_width = W;
-    uint32_t* panel_off = nullptr;
-    if (P > 1) {
-        panel_off = ar.alloc<uint32_t>(nfib * (uint64_t)(P + 1));
-        launch_panel_offsets(b_col, b_fib, fib_start, nb, P, log2w, panel_off, st);
-    }
-
-    Operands op;
-    op.na = na; op.nb = nb; op.nrows = nrows; op.ncols = ncols; op.nfib = nfib;
+    Front F;
+    Operands& op = F.op;
+    op.na = na; op.nb = nb; op.nrows = rows.nruns; op.ncols = ncols; op.nfib = fib.n;
     op.fa = fa; op.fb = fb;
     op.a_val = a_val; op.a_fib = a_fib; op.row_start = rows.run_start;
-    op.b_col = b_col; op.b_val = b_val; op.fib_start = fib_start;
+    op.b_col = fib.col; op.b_val = fib.val; op.fib_start = fib.start;
     op.row_tuple = row_tuple; op.col_tuple = col_tuple;
-    op.panel_off = panel_off; op.npanels = P; op.panel_log2 = log2w;
     op.err = err;
+    F.b_fib = fib.of;
+    F.a_row = rows.run_of;
+    F.h_row_first = {0u, (uint32_t)rows.nruns};
+    F.row_first = ar.alloc<uint32_t>(2);
+    PTC_CUDA(cudaMemcpyAsync(F.row_first, F.h_row_first.data(), 2 * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    F.colbase = {0u};
+    F.item_fa = {fa};
+    F.item_fb = {fb};
+    stats.ncols = ncols;
+    return F;
+}
 
-    // row classes and work lists (largest rows first)
-    uint32_t* small_flag = ar.alloc<uint32_t>(nrows + 1);
-    uint32_t* big_flag = ar.alloc<uint32_t>(nrows + 1);
-    uint32_t* esc_flag = ar.alloc<uint32_t>(nrows + 1);
-    launch_classify_rows(row_flops, rows.run_start, nrows, small_row_max_flops(), kEscMaxAvgProducts, small_flag,
-                         big_flag, esc_flag, st);
-    uint32_t* esc_pos = ar.alloc<uint32_t>(nrows + 1);
-    exclusive_scan<uint32_t>(esc_flag, esc_pos, nrows, ar);
-    uint32_t n_esc = read_scalar(esc_pos + nrows, st);
-    uint32_t* esc_rows = ar.alloc<uint32_t>(n_esc);
-    launch_compact_indices(esc_flag, esc_pos, nrows, esc_rows, st);
-    uint64_t* esc_off = ar.alloc<uint64_t>((uint64_t)n_esc + 1);
-    uint64_t f_esc = 0;
-    if (n_esc > 0) {
-        launch_esc_len(esc_rows, n_esc, row_flops, esc_off, st);
-        exclusive_scan<uint64_t>(esc_off, esc_off, n_esc, ar);
-        f_esc = read_scalar(esc_off + n_esc, st);
-        const int ebits = bits_for_space((uint64_t)n_esc), cbits2 = bits_for_space(std::max<uint64_t>(ncols, 1));
-        if (f_esc > kEscMaxProducts || ebits + cbits2 > 64) {  // too large for the sort buffers: hash path
-            launch_merge_flags(big_flag, esc_flag, nrows, st);
-            n_esc = 0;
-            f_esc = 0;
-        }
-    }
-    uint32_t* small_pos = ar.alloc<uint32_t>(nrows + 1);
-    uint32_t* big_pos = ar.alloc<uint32_t>(nrows + 1);
-    exclusive_scan<uint32_t>(small_flag, small_pos, nrows, ar);
-    exclusive_scan<uint32_t>(big_flag, big_pos, nrows, ar);
-    const uint32_t n_small = read_scalar(small_pos + nrows, st);
-    const uint32_t n_big = read_scalar(big_pos + nrows, st);
-    uint32_t* small_rows = ar.alloc<uint32_t>(n_small);
-    uint32_t* big_rows = ar.alloc<uint32_t>(n_big);
-    launch_compact_indices(small_flag, small_pos, nrows, small_rows, st);
-    launch_compact_indices(big_flag, big_pos, nrows, big_rows, st);
-    if (n_big > 1) {
-        uint64_t* wkey = ar.alloc<uint64_t>(n_big);
-        launch_work_keys(big_rows, n_big, row_flops, wkey, st);
-        radix_sort_pairs(wkey, big_rows, n_big, 0, 40, ar);
-    }
-    stats.rows_small = n_small;
-    stats.rows_hash = n_big;
-    stats.rows_long = n_esc;
+void contract_impl(const ptc_coo* A, const ptc_coo* Bin, uint32_t c, const uint32_t* a_modes,
+                   const uint32_t* b_modes_in, const ptc_options* opt_in, ptc_tensor* out, ptc_stats* stats_out,
+                   Collect* collect = nullptr) {
+    const ptc_options opt = resolve_options(opt_in);
+    PTC_REQUIRE(out != nullptr, PTC_ERR_INVALID_ARGUMENT, "out is null");
+    std::memset(out, 0, sizeof(*out));
+    ptc_stats stats;
+    std::memset(&stats, 0, sizeof(stats));
+    g_launches = 0;
+
+    const bool self = (Bin == nullptr);
+    const ptc_coo* B = self ? A : Bin;
+    const uint32_t* b_modes = self ? a_modes : b_modes_in;
+    validate_pair(A, B, c, a_modes, b_modes, "");
+    if (self) PTC_REQUIRE(A->nnz > 1, PTC_ERR_TOO_FEW_NONZEROS, "Tensor B has at most one nonzeros");
+    const uint32_t fa = A->order - c, fb = B->order - c;
+
+    DeviceSetup dev = setup_device(opt);
+    cudaStream_t st = dev.stream;
+    Events ev;
+    Arena ar(st);
+    PTC_CUDA(cudaEventRecord(ev.ev[EV_START], st));
+    const Knobs kn = knobs_of(opt);
+    Front F = front_single(A, B, self, c, a_modes, b_modes, opt, kn, ar, ev, stats);
 
     const bool learned = opt.path == PTC_PATH_LEARNED && collect == nullptr;
     const SizerHost* sizer = nullptr;
@@ -625,125 +905,48 @@ void contract_impl(const ptc_coo* A, const ptc_coo* Bin, uint32_t c, const uint3
         PTC_REQUIRE(sizer != nullptr, PTC_ERR_INVALID_ARGUMENT,
                     "the learned path needs a sizer: opt.sizer, or sizer_default.bin beside the library");
     }
-    SplitRule rule;
-    rule.cap = hash_part_capacity();
-    rule.dense_panels = dense_part_columns() >> log2w;
-    rule.dense_min = W / kDenseMinFraction;
-    rule.min_bits = hash_part_min_bits();
-
-    // symbolic: exact output nnz per row (and per fine panel for the large rows); the learned
-    // path counts only the sort-based rows (their sort gives the counts) and predicts the rest
-    uint64_t* row_d = ar.alloc<uint64_t>(nrows + 1);
-    PTC_CUDA(cudaMemsetAsync(row_d, 0, (nrows + 1) * sizeof(uint64_t), st));
-    uint32_t* panel_cnt = ar.alloc<uint32_t>((uint64_t)n_big * P);
-    uint32_t* work_counter = ar.alloc<uint32_t>(1);
-    OutputView none;
-    if (!learned) {
-        launch_small_rows(false, op, small_rows, n_small, row_d, nullptr, none, st);
-        launch_sym_bitmap(op, big_rows, n_big, panel_cnt, row_d, work_counter, num_sms, st);
-    }
-    // sort-based rows: expand their products in stream order, sort stably by (row, column)
-    const uint32_t esc_colbits = (uint32_t)colbits;
-    uint64_t* esc_key = nullptr;
-    double* esc_val = nullptr;
-    uint32_t* esc_perm = nullptr;
-    uint32_t* esc_run_start = nullptr;
-    uint64_t* esc_run_key = nullptr;
-    uint32_t* esc_first = nullptr;
-    uint64_t esc_runs = 0;
-    if (n_esc > 0) {
-        int32_t* esc_of = ar.alloc<int32_t>(nrows);
-        PTC_CUDA(cudaMemsetAsync(esc_of, 0xff, nrows * sizeof(int32_t), st));
-        launch_esc_index(esc_rows, n_esc, esc_of, st);
-        esc_key = ar.alloc<uint64_t>(f_esc);
-        esc_val = ar.alloc<double>(f_esc);
-        esc_perm = ar.alloc<uint32_t>(f_esc);
-        launch_esc_expand(op, rows.run_of, esc_of, alen, esc_off, esc_colbits, esc_key, esc_val, esc_perm, st);
-        radix_sort_pairs(esc_key, esc_perm, f_esc, 0, esc_colbits + bits_for_space((uint64_t)n_esc), ar);
-        esc_run_start = ar.alloc<uint32_t>(f_esc + 1);
-        esc_run_key = ar.alloc<uint64_t>(f_esc);
-        esc_runs = runs_of_sorted(esc_key, f_esc, nullptr, esc_run_start, esc_run_key, ar);
-        esc_first = ar.alloc<uint32_t>(n_esc);
-        launch_esc_count(esc_run_key, esc_runs, esc_colbits, esc_rows, row_d, esc_first, st);
-    }
-    uint64_t* row_off = ar.alloc<uint64_t>(nrows + 1);
-    exclusive_scan<uint64_t>(row_d, row_off, nrows, ar);
-    const uint64_t exact_nnz = read_scalar(row_off + nrows, st);  // all rows, or sort-based rows only
-    if (collect) {
-        // features of the rows the learned path sizes, and log2(1 + their exact output nnz)
-        float* gp = ar.alloc<float>((uint64_t)(P + 1) * kGridPoints);
-        launch_popularity_table(b_col, nb, ncols, P, log2w, gp, ar);
-        float* fx = ar.alloc<float>((uint64_t)n_big * kSizerInputs);
-        float* ft = ar.alloc<float>(n_big);
-        launch_row_features(op, big_rows, n_big, row_flops, gp, fx, st);
-        launch_row_targets(big_rows, n_big, row_d, ft, st);
-        collect->x.resize((uint64_t)n_big * kSizerInputs);
-        collect->t.resize(n_big);
-        PTC_CUDA(cudaMemcpyAsync(collect->x.data(), fx, collect->x.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
-        PTC_CUDA(cudaMemcpyAsync(collect->t.data(), ft, collect->t.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+    Plan pl = plan_rows(F, opt, sizer, collect, dev.num_sms, ar, stats);
+    PTC_REQUIRE(pl.flops > 0, PTC_ERR_EMPTY_CONTRACTION, "tensor contraction not possible!! (no matching fibers)");
+    if (pl.collected) {
         ar.release();
         PTC_CUDA(cudaStreamSynchronize(st));
-        stats.out_nnz = exact_nnz;
+        stats.out_nnz = pl.exact_nnz;
         if (stats_out) *stats_out = stats;
         return;
     }
-
-    float* pred = nullptr;
-    uint64_t capacity = exact_nnz;
-    if (learned && n_big > 0) {
-        // sizer: per-row features -> predicted log2(1 + nnz) -> per-panel counts by column popularity
-        float* gp = ar.alloc<float>((uint64_t)(P + 1) * kGridPoints);
-        launch_popularity_table(b_col, nb, ncols, P, log2w, gp, ar);
-        float* fx = ar.alloc<float>((uint64_t)n_big * kSizerInputs);
-        launch_row_features(op, big_rows, n_big, row_flops, gp, fx, st);
-        pred = ar.alloc<float>(n_big);
-        sizer_predict_device(*sizer, fx, n_big, pred, ar);
-        launch_predicted_panel_counts(big_rows, n_big, row_flops, pred, gp, P, log2w, ncols, kSizerMargin, panel_cnt,
-                                      st);
-        uint64_t* psum = ar.alloc<uint64_t>(1);
-        launch_sum_u32(panel_cnt, (uint64_t)n_big * P, psum, st);
-        capacity += read_scalar(psum, st);
-    }
-    if (learned) capacity += (uint64_t)n_small * small_row_max_flops() + 1024;
-
-    // split large rows into parts that fit a shared-memory table
-    uint32_t* nparts = ar.alloc<uint32_t>((uint64_t)n_big + 1);
-    launch_count_parts(panel_cnt, n_big, P, rule, nparts, err, st);
-    exclusive_scan<uint32_t>(nparts, nparts, n_big, ar);
-    const uint32_t n_parts = read_scalar(nparts + n_big, st);
-    PTC_REQUIRE(read_scalar(err, st) == 0, PTC_ERR_INTERNAL, "a fine panel exceeds the hash part capacity");
-    PartItem* parts = ar.alloc<PartItem>(n_parts);
-    launch_fill_parts(big_rows, panel_cnt, n_big, P, rule, nparts, learned ? nullptr : row_off, parts, st);
-    stats.hash_parts = n_parts;
     PTC_CUDA(cudaEventRecord(ev.ev[EV_SYM], st));
+    const Operands& op = F.op;
 
     // ---- numeric ----
     const uint32_t od = fa + fb;
+    const uint64_t capacity = learned ? pl.exact_nnz + pl.claim_total + 1024 : pl.exact_nnz;
     OutputView ov;
     PTC_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&ov.idx), std::max<uint64_t>(capacity * od, 1) * sizeof(uint32_t), st));
     PTC_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&ov.val), std::max<uint64_t>(capacity, 1) * sizeof(double), st));
-    uint64_t out_nnz = exact_nnz;
+    uint64_t out_nnz = pl.exact_nnz;
     try {
         if (learned) {
+            // the small and sort-based rows fill [0, exact_nnz); the large rows claim after them
             ov.capacity = capacity;
             ov.cursor = ar.alloc<uint64_t>(1);
+            ov.overshoot = ar.alloc<uint64_t>(1);
             ov.fail_count = ar.alloc<uint32_t>(1);
-            ov.fail_list = ar.alloc<uint32_t>(std::max<uint32_t>(n_parts, 1));
-            ov.item_count = ar.alloc<uint32_t>(std::max<uint32_t>(n_parts, 1));
-            PTC_CUDA(cudaMemcpyAsync(ov.cursor, &exact_nnz, sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+            ov.fail_list = ar.alloc<uint32_t>(std::max<uint32_t>(pl.n_parts, 1));
+            ov.item_count = ar.alloc<uint32_t>(std::max<uint32_t>(pl.n_parts, 1));
+            PTC_CUDA(cudaMemcpyAsync(ov.cursor, &pl.exact_nnz, sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+            PTC_CUDA(cudaMemsetAsync(ov.overshoot, 0, sizeof(uint64_t), st));
             PTC_CUDA(cudaMemsetAsync(ov.fail_count, 0, sizeof(uint32_t), st));
         }
-        launch_small_rows(true, op, small_rows, n_small, nullptr, learned ? nullptr : row_off, ov, st);
-        launch_hash_parts(op, parts, n_parts, ov, work_counter, err, num_sms, st);
-        if (n_esc > 0)
-            launch_esc_fold(op, ov, esc_run_key, esc_run_start, esc_runs, esc_colbits, esc_rows, esc_first, row_off,
-                            esc_perm, esc_val, f_esc, reinterpret_cast<double*>(esc_key), st);
+        launch_small_rows(true, op, pl.small_rows, pl.n_small, nullptr, pl.row_off, ov, st);
+        launch_hash_parts(op, pl.parts, pl.n_parts, ov, pl.work_counter, op.err, dev.num_sms, st);
+        launch_esc_fold(op, ov, pl.esc_run_key, pl.esc_run_start, 0, pl.esc_runs, pl.esc_colbits, pl.esc_rows,
+                        pl.esc_first, pl.row_off, pl.esc_sorted, st);
         if (learned) {
-            out_nnz = learned_reruns(op, parts, n_parts, big_rows, n_big, pred, rule, ov, work_counter, err, num_sms,
-                                     nrows, ar, stats);
+            out_nnz = learned_reruns(op, pl.parts, pl.n_parts, pl.big_rows, pl.n_big, pl.pred, pl.rule, ov,
+                                     pl.work_counter, op.err, dev.num_sms, op.nrows, ar, stats);
         }
         PTC_CUDA(cudaEventRecord(ev.ev[EV_NUM], st));
-        PTC_REQUIRE(read_scalar(err, st) == 0, PTC_ERR_INTERNAL,
+        PTC_REQUIRE(read_scalar(op.err, st) == 0, PTC_ERR_INTERNAL,
                     "an accumulator table overflowed or met an out-of-range column");
     } catch (...) {
         cudaFreeAsync(ov.idx, st);
@@ -792,6 +995,620 @@ void contract_impl(const ptc_coo* A, const ptc_coo* Bin, uint32_t c, const uint3
     stats.kernel_launches = g_launches;
     if (opt.verbose) print_reference_lines(stats);
     if (stats_out) *stats_out = stats;
+}
+
+// ---------------------------------------------------------------------------------------------
+// batches: many contractions as one problem
+// ---------------------------------------------------------------------------------------------
+//
+// Every item's keys are offset into a key range of its own (contracted keys by the sizes of the
+// earlier items' contracted key spaces, free keys likewise), so one pass of each kernel -- keys,
+// sorts, one cuckoo table, symbolic pass, accumulators -- serves the whole batch, and rows and
+// columns of different items never meet.  Column ids stay local to their item (the accumulators
+// index tables by them); the items' rows are contiguous in row order.  The output of the batch is
+// produced in waves of consecutive items whose outputs fit a device budget; each wave's numeric
+// pass is one CUDA-graph launch.
+
+// Output block of one wave, shared by the item tensors cut from it (ptc_tensor::opaque); the last
+// ptc_tensor_free of them releases it.
+struct SharedBlock {
+    std::atomic<uint32_t> refs{0};
+    uint32_t location = PTC_HOST;
+    void* idx = nullptr;
+    void* val = nullptr;
+};
+
+void release_block(SharedBlock* b) {
+    if (b->refs.fetch_sub(1) != 1) return;
+    if (b->location == PTC_DEVICE) {
+        cudaFree(b->idx);
+        cudaFree(b->val);
+    } else {
+        std::free(b->idx);
+        std::free(b->val);
+    }
+    delete b;
+}
+
+struct BatchItemHost {
+    const ptc_coo* A;
+    const ptc_coo* B;
+    bool self;
+    uint32_t c;
+    const uint32_t* a_modes;
+    const uint32_t* b_modes;
+    uint32_t fa, fb;
+};
+
+// Where the items' outputs go: outs[id] (kept), sink(user, id, view) (streamed), or nowhere.
+struct BatchTarget {
+    ptc_tensor* outs = nullptr;
+    ptc_batch_sink sink = nullptr;
+    void* user = nullptr;
+    std::vector<uint32_t> ids;  // caller's index of each item
+};
+
+void fill_side(ItemSide& s, const ptc_coo* t, const uint32_t* modes, const KeySpec& con, const KeySpec& fr,
+               uint64_t fbase) {
+    s.order = t->order;
+    s.fbase = fbase;
+    for (uint32_t j = 0; j < t->order; ++j) {
+        s.mode[j] = modes[j];
+        s.dim[j] = t->dims[j];
+        s.stride[j] = j < con.n ? con.stride[j] : fr.stride[j - con.n];
+    }
+}
+
+Front front_batch(const std::vector<BatchItemHost>& items, uint32_t location, const ptc_options& opt, const Knobs& kn,
+                  Arena& ar, Events& ev, ptc_stats& stats) {
+    cudaStream_t st = ar.stream();
+    const uint32_t n = (uint32_t)items.size();
+    std::vector<ItemSpec> spec(n);
+    std::vector<uint64_t> a_off(n + 1, 0), b_off(n + 1, 0), abase(n), bbase(n);
+    unsigned __int128 cb = 0, ab = 0, bb = 0;
+    bool all_self = true;
+    uint32_t fa_w = 0, fb_w = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        const BatchItemHost& x = items[i];
+        const KeySpec ac = make_keyspec(x.A->dims, x.a_modes, x.c);
+        const KeySpec af = make_keyspec(x.A->dims, x.a_modes + x.c, x.fa);
+        const KeySpec bc = make_keyspec(x.B->dims, x.b_modes, x.c);
+        const KeySpec bf = make_keyspec(x.B->dims, x.b_modes + x.c, x.fb);
+        ItemSpec& s = spec[i];
+        std::memset(&s, 0, sizeof(s));
+        s.cbase = (uint64_t)cb;
+        s.c = x.c;
+        fill_side(s.side[0], x.A, x.a_modes, ac, af, (uint64_t)ab);
+        fill_side(s.side[1], x.B, x.b_modes, bc, bf, (uint64_t)bb);
+        abase[i] = (uint64_t)ab;
+        bbase[i] = (uint64_t)bb;
+        cb += ac.space;
+        ab += af.space;
+        bb += bf.space;
+        PTC_REQUIRE(cb <= (unsigned __int128)UINT64_MAX && ab <= (unsigned __int128)UINT64_MAX &&
+                        bb <= (unsigned __int128)UINT64_MAX,
+                    PTC_ERR_KEY_OVERFLOW, "the batch's key spaces together do not fit in 64 bits");
+        a_off[i + 1] = a_off[i] + x.A->nnz;
+        b_off[i + 1] = b_off[i] + x.B->nnz;
+        all_self = all_self && x.self;
+        fa_w = std::max(fa_w, x.fa);
+        fb_w = std::max(fb_w, x.fb);
+    }
+    const uint64_t na = a_off[n], nb = all_self ? na : b_off[n];
+    PTC_REQUIRE(na < (1ull << 32) && nb < (1ull << 32), PTC_ERR_INVALID_ARGUMENT,
+                "a batch holds fewer than 2^32 nonzeros per side");
+
+    // ---- inputs on the device: host items are staged into one buffer per side ----
+    if (location == PTC_HOST) {
+        for (int side = 0; side < 2; ++side) {
+            if (side == 1 && all_self) break;
+            uint64_t words = 0, vals = 0;
+            for (uint32_t i = 0; i < n; ++i) {
+                const ptc_coo* t = side == 0 ? items[i].A : items[i].B;
+                if (side == 1 && items[i].self) continue;
+                words += t->nnz * t->order;
+                vals += t->nnz;
+            }
+            uint32_t* didx = ar.alloc<uint32_t>(words);
+            double* dval = ar.alloc<double>(vals);
+            std::vector<HostSeg> si, sv;
+            uint64_t wo = 0, vo = 0;
+            for (uint32_t i = 0; i < n; ++i) {
+                const ptc_coo* t = side == 0 ? items[i].A : items[i].B;
+                if (side == 1 && items[i].self) continue;
+                spec[i].side[side].idx = didx + wo;
+                spec[i].side[side].vals = dval + vo;
+                si.push_back({t->idx, t->nnz * t->order * sizeof(uint32_t)});
+                sv.push_back({t->vals, t->nnz * sizeof(double)});
+                wo += t->nnz * t->order;
+                vo += t->nnz;
+            }
+            host_copier().gather_to_device(didx, si, st);
+            host_copier().gather_to_device(dval, sv, st);
+        }
+        for (uint32_t i = 0; i < n; ++i)
+            if (items[i].self) {
+                spec[i].side[1].idx = spec[i].side[0].idx;
+                spec[i].side[1].vals = spec[i].side[0].vals;
+            }
+    } else {
+        for (uint32_t i = 0; i < n; ++i) {
+            spec[i].side[0].idx = items[i].A->idx;
+            spec[i].side[0].vals = items[i].A->vals;
+            spec[i].side[1].idx = items[i].B->idx;
+            spec[i].side[1].vals = items[i].B->vals;
+        }
+    }
+    PTC_CUDA(cudaEventRecord(ev.ev[EV_H2D], st));
+    stats.a_nnz = na;
+    stats.b_nnz = nb;
+
+    auto upload = [&](const auto& v) {
+        using T = typename std::decay_t<decltype(v)>::value_type;
+        T* d = ar.alloc<T>(v.size());
+        PTC_CUDA(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+        return d;
+    };
+    const ItemSpec* specs_d = upload(spec);
+    const uint64_t* a_off_d = upload(a_off);
+    const uint64_t* b_off_d = all_self ? a_off_d : upload(b_off);
+    const uint64_t* abase_d = upload(abase);
+    const uint64_t* bbase_d = all_self ? abase_d : upload(bbase);
+
+    // ---- keys ----
+    uint32_t* err = ar.alloc<uint32_t>(1);
+    PTC_CUDA(cudaMemsetAsync(err, 0, sizeof(uint32_t), st));
+    uint64_t* a_ckey = ar.alloc<uint64_t>(na);
+    uint64_t* a_fkey = ar.alloc<uint64_t>(na);
+    double* a_vals = ar.alloc<double>(na);
+    launch_pack_items(specs_d, a_off_d, n, 0, na, a_ckey, a_fkey, a_vals, err, st);
+    uint64_t* b_ckey = a_ckey;
+    uint64_t* b_fkey = a_fkey;
+    double* b_vals = a_vals;
+    if (!all_self) {
+        b_ckey = ar.alloc<uint64_t>(nb);
+        b_fkey = ar.alloc<uint64_t>(nb);
+        b_vals = ar.alloc<double>(nb);
+        launch_pack_items(specs_d, b_off_d, n, 1, nb, b_ckey, b_fkey, b_vals, err, st);
+    }
+    PTC_REQUIRE(read_scalar(err, st) == 0, PTC_ERR_INDEX_RANGE, "an index is not smaller than its mode size");
+
+    // ---- B side: columns (global ranks, then local to their item), fibers, cuckoo table ----
+    Ranked cols = rank_keys(b_fkey, nb, (uint64_t)bb, ar);
+    uint32_t* col_first = ar.alloc<uint32_t>(n + 1);
+    launch_key_bounds(cols.run_key, cols.nruns, bbase_d, n, col_first, st);
+    std::vector<uint32_t> h_col_first(n + 1);
+    PTC_CUDA(cudaMemcpyAsync(h_col_first.data(), col_first, (n + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    uint32_t* col_local = ar.alloc<uint32_t>(nb);
+    launch_localize(cols.rank_of, nb, b_off_d, n, col_first, col_local, st);
+    uint32_t* col_tuple = ar.alloc<uint32_t>(cols.nruns * std::max(fb_w, 1u));
+    launch_item_tuples(cols.run_start, cols.perm, cols.nruns, specs_d, b_off_d, n, 1, fb_w, col_tuple, st);
+    Fibers fib = group_fibers(b_ckey, cols.rank_of, cols.nruns, nb, bits_for_space((uint64_t)cb), b_vals, ar,
+                              col_local);
+    CuckooBuildInfo cinfo;
+    const CuckooTable table = cuckoo_build(fib.key, fib.n, opt.hash_seed, 64, kn.max_load, 8, ar, &cinfo);
+    stats.hash_attempts = cinfo.attempts;
+    PTC_CUDA(cudaEventRecord(ev.ev[EV_BSIDE], st));
+    PTC_CUDA(cudaStreamSynchronize(st));  // h_col_first
+    uint64_t ncols_local = 0;
+    for (uint32_t i = 0; i < n; ++i) ncols_local = std::max<uint64_t>(ncols_local, h_col_first[i + 1] - h_col_first[i]);
+
+    // ---- A side ----
+    Ranked rows;
+    uint32_t* row_first = col_first;
+    uint32_t* row_tuple = col_tuple;
+    if (all_self) {
+        rows = cols;
+    } else {
+        rows = rank_keys(a_fkey, na, (uint64_t)ab, ar);
+        row_first = ar.alloc<uint32_t>(n + 1);
+        launch_key_bounds(rows.run_key, rows.nruns, abase_d, n, row_first, st);
+        row_tuple = ar.alloc<uint32_t>(rows.nruns * std::max(fa_w, 1u));
+        launch_item_tuples(rows.run_start, rows.perm, rows.nruns, specs_d, a_off_d, n, 0, fa_w, row_tuple, st);
+    }
+    Front F;
+    F.h_row_first.resize(n + 1);
+    PTC_CUDA(cudaMemcpyAsync(F.h_row_first.data(), row_first, (n + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    uint32_t* row_item = ar.alloc<uint32_t>(std::max<uint64_t>(rows.nruns, 1));
+    launch_row_item(rows.nruns, row_first, n, row_item, st);
+    uint64_t* a_ckey_sorted = ar.alloc<uint64_t>(na);
+    double* a_val = ar.alloc<double>(na);
+    launch_gather<uint64_t>(a_ckey, rows.perm, na, a_ckey_sorted, st);
+    launch_gather<double>(a_vals, rows.perm, na, a_val, st);
+    int32_t* a_fib = ar.alloc<int32_t>(na);
+    cuckoo_lookup(table, a_ckey_sorted, na, a_fib, ar);
+    PTC_CUDA(cudaEventRecord(ev.ev[EV_ASIDE], st));
+    PTC_CUDA(cudaStreamSynchronize(st));  // h_row_first
+
+    Operands& op = F.op;
+    op.na = na; op.nb = nb; op.nrows = rows.nruns; op.ncols = ncols_local; op.nfib = fib.n;
+    op.fa = fa_w; op.fb = fb_w;
+    op.a_val = a_val; op.a_fib = a_fib; op.row_start = rows.run_start;
+    op.b_col = fib.col; op.b_val = fib.val; op.fib_start = fib.start;
+    op.row_tuple = row_tuple; op.col_tuple = col_tuple;
+    op.err = err;
+    op.row_item = row_item;
+    F.item_out = ar.alloc<ItemOut>(n);
+    op.item_out = F.item_out;
+    F.b_fib = fib.of;
+    F.a_row = rows.run_of;
+    F.batch = true;
+    F.nitems = n;
+    F.row_first = row_first;
+    F.colbase = h_col_first;
+    F.item_fa.resize(n);
+    F.item_fb.resize(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        F.item_fa[i] = items[i].fa;
+        F.item_fb[i] = items[i].fb;
+    }
+    stats.ncols = cols.nruns;
+    return F;
+}
+
+// values of a device array at the given indices, on the host
+template <typename T>
+std::vector<T> read_at(const T* a, const std::vector<uint32_t>& at, Arena& ar) {
+    cudaStream_t st = ar.stream();
+    uint32_t* at_d = ar.alloc<uint32_t>(at.size());
+    T* v_d = ar.alloc<T>(at.size());
+    PTC_CUDA(cudaMemcpyAsync(at_d, at.data(), at.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    launch_gather<T>(a, at_d, at.size(), v_d, st);
+    std::vector<T> v(at.size());
+    PTC_CUDA(cudaMemcpyAsync(v.data(), v_d, v.size() * sizeof(T), cudaMemcpyDeviceToHost, st));
+    PTC_CUDA(cudaStreamSynchronize(st));
+    return v;
+}
+
+void deliver_empty(const BatchTarget& tg, uint32_t i, const BatchItemHost& x, uint32_t location) {
+    ptc_tensor t;
+    std::memset(&t, 0, sizeof(t));
+    t.order = x.fa + x.fb;
+    t.location = location;
+    if (tg.outs) tg.outs[tg.ids[i]] = t;
+    if (tg.sink) tg.sink(tg.user, tg.ids[i], &t);
+}
+
+void batch_impl(const std::vector<BatchItemHost>& items, uint32_t location, const ptc_options& opt, bool exact_only,
+                const BatchTarget& tg, ptc_stats& stats) {
+    const uint32_t n = (uint32_t)items.size();
+    DeviceSetup dev = setup_device(opt);
+    cudaStream_t st = dev.stream;
+    Events ev;
+    Arena ar(st);
+    PTC_CUDA(cudaEventRecord(ev.ev[EV_START], st));
+    const Knobs kn = knobs_of(opt);
+    Front F = front_batch(items, location, opt, kn, ar, ev, stats);
+
+    const bool learned = opt.path == PTC_PATH_LEARNED && !exact_only;
+    const SizerHost* sizer = nullptr;
+    if (learned) {
+        sizer = opt.sizer ? sizer_host(opt.sizer) : default_sizer();
+        PTC_REQUIRE(sizer != nullptr, PTC_ERR_INVALID_ARGUMENT,
+                    "the learned path needs a sizer: opt.sizer, or sizer_default.bin beside the library");
+    }
+    Plan pl = plan_rows(F, opt, sizer, nullptr, dev.num_sms, ar, stats);
+    const Operands& op = F.op;
+    const uint64_t nrows = op.nrows;
+    if (pl.flops == 0) {
+        for (uint32_t i = 0; i < n; ++i) deliver_empty(tg, i, items[i], opt.output_location);
+        ar.release();
+        PTC_CUDA(cudaStreamSynchronize(st));
+        return;
+    }
+
+    // ---- each item's range of entries: [E_i, E_i + S_i) ----
+    // two-phase: exact counts; learned: the small and sort-based rows' exact entries first, then
+    // the large rows' claims within their predicted budgets
+    const std::vector<uint32_t>& rf = F.h_row_first;
+    const std::vector<uint64_t> ex = read_at<uint64_t>(pl.row_off, rf, ar);
+    std::vector<uint64_t> cl(n + 1, 0);
+    if (learned) {
+        cl = read_at<uint64_t>(pl.claim_off, rf, ar);
+        launch_shift_exact(nrows, op.row_item, F.row_first, pl.claim_off, pl.row_off, st);
+    }
+    std::vector<uint64_t> E(n + 1), S(n), X(n);
+    for (uint32_t i = 0; i <= n; ++i) E[i] = ex[i] + cl[i];
+    for (uint32_t i = 0; i < n; ++i) {
+        S[i] = E[i + 1] - E[i];
+        X[i] = ex[i + 1] - ex[i];
+    }
+    PTC_CUDA(cudaEventRecord(ev.ev[EV_SYM], st));
+
+    // ---- waves of consecutive items whose outputs fit the budget ----
+    const bool keep_device = tg.outs && opt.output_location == PTC_DEVICE;
+    uint64_t budget = (uint64_t)opt.batch_wave_mib << 20;
+    if (budget == 0) {
+        size_t free_b = 0, total_b = 0;
+        PTC_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        budget = (uint64_t)(free_b * 0.6);
+    }
+    if (keep_device) budget = UINT64_MAX;  // every output stays: one wave
+    std::vector<uint32_t> wave_item{0};
+    {
+        uint64_t acc = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            const uint64_t b = S[i] * (8 + 4ull * (items[i].fa + items[i].fb));
+            if (acc > 0 && acc + b > budget) {
+                wave_item.push_back(i);
+                acc = 0;
+            }
+            acc += b;
+        }
+        wave_item.push_back(n);
+    }
+    const uint32_t nw = (uint32_t)wave_item.size() - 1;
+    stats.batch_waves = nw;
+
+    // work of each wave: parts sorted by wave (largest first inside a wave), small rows, runs
+    std::vector<uint32_t> wave_row(nw + 1);
+    for (uint32_t w = 0; w <= nw; ++w) wave_row[w] = rf[wave_item[w]];
+    std::vector<uint32_t> pb(nw + 1, 0);
+    pb[nw] = pl.n_parts;
+    PartItem* parts = pl.parts;
+    if (nw > 1 && pl.n_parts > 0) {
+        uint32_t* wave_row_d = ar.alloc<uint32_t>(nw + 1);
+        PTC_CUDA(cudaMemcpyAsync(wave_row_d, wave_row.data(), (nw + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        uint64_t* key = ar.alloc<uint64_t>(pl.n_parts);
+        uint32_t* idx = ar.alloc<uint32_t>(pl.n_parts);
+        launch_part_wave(pl.parts, pl.n_parts, wave_row_d, nw, key, idx, st);
+        radix_sort_pairs(key, idx, pl.n_parts, 0, bits_for_space(nw), ar);
+        parts = ar.alloc<PartItem>(pl.n_parts);
+        launch_gather_parts(pl.parts, idx, pl.n_parts, parts, st);
+        std::vector<uint64_t> wid(nw);
+        for (uint32_t w = 0; w < nw; ++w) wid[w] = w;
+        uint64_t* wid_d = ar.alloc<uint64_t>(nw);
+        PTC_CUDA(cudaMemcpyAsync(wid_d, wid.data(), nw * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+        uint32_t* bounds = ar.alloc<uint32_t>(nw + 1);
+        launch_key_bounds(key, pl.n_parts, wid_d, nw, bounds, st);
+        PTC_CUDA(cudaMemcpyAsync(pb.data(), bounds, (nw + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        PTC_CUDA(cudaStreamSynchronize(st));
+    }
+    const std::vector<uint32_t> sb = read_at<uint32_t>(pl.small_pos, wave_row, ar);
+    std::vector<uint32_t> rb(nw + 1, 0);
+    if (pl.n_esc > 0) rb = read_at<uint32_t>(pl.esc_first, read_at<uint32_t>(pl.esc_pos, wave_row, ar), ar);
+
+    // learned: the claim cursors of every item
+    OutputView base;
+    if (learned) {
+        std::vector<uint64_t> cur(n), end(n);
+        for (uint32_t i = 0; i < n; ++i) {
+            cur[i] = E[i] + X[i];
+            end[i] = E[i] + S[i];
+        }
+        base.cursor = ar.alloc<uint64_t>(n);
+        base.overshoot = ar.alloc<uint64_t>(n);
+        uint64_t* end_d = ar.alloc<uint64_t>(n);
+        PTC_CUDA(cudaMemcpyAsync(base.cursor, cur.data(), n * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+        PTC_CUDA(cudaMemcpyAsync(end_d, end.data(), n * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+        PTC_CUDA(cudaMemsetAsync(base.overshoot, 0, n * sizeof(uint64_t), st));
+        base.cap_end = end_d;
+        base.fail_count = ar.alloc<uint32_t>(1);
+        base.fail_list = ar.alloc<uint32_t>(std::max<uint32_t>(pl.n_parts, 1));
+        PTC_CUDA(cudaStreamSynchronize(st));  // the host vectors above go out of scope
+    }
+
+    // output blocks: one per wave when the outputs are kept on the device, else one reused block
+    uint64_t max_vals = 0, max_words = 0;
+    std::vector<uint64_t> wave_vals(nw, 0), wave_words(nw, 0);
+    for (uint32_t w = 0; w < nw; ++w) {
+        for (uint32_t i = wave_item[w]; i < wave_item[w + 1]; ++i) {
+            wave_vals[w] += S[i];
+            wave_words[w] += S[i] * (items[i].fa + items[i].fb);
+        }
+        max_vals = std::max(max_vals, wave_vals[w]);
+        max_words = std::max(max_words, wave_words[w]);
+    }
+    uint32_t* blk_idx = nullptr;
+    double* blk_val = nullptr;
+    void* host_blk_idx = nullptr;
+    void* host_blk_val = nullptr;
+    auto free_blocks = [&]() {  // blocks handed to the caller are no longer held here
+        if (blk_idx) cudaFreeAsync(blk_idx, st);
+        if (blk_val) cudaFreeAsync(blk_val, st);
+        std::free(host_blk_idx);
+        std::free(host_blk_val);
+        blk_idx = nullptr;
+        blk_val = nullptr;
+        host_blk_idx = host_blk_val = nullptr;
+    };
+    std::vector<uint8_t> failed(n, 0);
+    double t_numeric = 0.0, t_out = 0.0;
+    try {
+        if (!keep_device) {
+            PTC_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&blk_idx), std::max<uint64_t>(max_words, 1) * 4, st));
+            PTC_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&blk_val), std::max<uint64_t>(max_vals, 1) * 8, st));
+        }
+        const bool host_view = opt.output_location == PTC_HOST && tg.sink && !tg.outs;
+        if (host_view) {
+            host_blk_idx = host_result_alloc(std::max<uint64_t>(max_words, 1) * 4);
+            host_blk_val = host_result_alloc(std::max<uint64_t>(max_vals, 1) * 8);
+            PTC_REQUIRE(host_blk_idx && host_blk_val, PTC_ERR_OUT_OF_MEMORY, "host output allocation failed");
+        }
+        std::vector<ItemOut> io(n);
+        for (uint32_t w = 0; w < nw; ++w) {
+            const uint32_t i0 = wave_item[w], i1 = wave_item[w + 1];
+            if (keep_device) {
+                PTC_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&blk_idx), std::max<uint64_t>(wave_words[w], 1) * 4, st));
+                PTC_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&blk_val), std::max<uint64_t>(wave_vals[w], 1) * 8, st));
+            }
+            uint64_t words = 0;
+            for (uint32_t i = i0; i < i1; ++i) {
+                io[i].ent0 = E[i];
+                io[i].val0 = E[i] - E[i0];
+                io[i].idx0 = words;
+                io[i].colbase = F.colbase[i];
+                io[i].fa = items[i].fa;
+                io[i].fb = items[i].fb;
+                io[i].pad = 0;
+                words += S[i] * (items[i].fa + items[i].fb);
+            }
+            PTC_CUDA(cudaMemcpyAsync(F.item_out + i0, io.data() + i0, (i1 - i0) * sizeof(ItemOut),
+                                     cudaMemcpyHostToDevice, st));
+            OutputView ov = base;
+            ov.idx = blk_idx;
+            ov.val = blk_val;
+            if (learned) PTC_CUDA(cudaMemsetAsync(ov.fail_count, 0, sizeof(uint32_t), st));
+            PTC_CUDA(cudaEventRecord(ev.ev[EV_WAVE0], st));
+            const bool work = sb[w + 1] > sb[w] || pb[w + 1] > pb[w] || rb[w + 1] > rb[w];
+            // the wave's numeric pass, captured and launched as one graph
+            cudaGraph_t graph = nullptr;
+            cudaGraphExec_t exec = nullptr;
+            if (work) {
+                PTC_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+                try {
+                    launch_small_rows(true, op, pl.small_rows + sb[w], sb[w + 1] - sb[w], nullptr, pl.row_off, ov,
+                                      st);
+                    launch_hash_parts(op, parts + pb[w], pb[w + 1] - pb[w], ov, pl.work_counter, op.err, dev.num_sms,
+                                      st);
+                    launch_esc_fold(op, ov, pl.esc_run_key, pl.esc_run_start, rb[w], rb[w + 1], pl.esc_colbits,
+                                    pl.esc_rows, pl.esc_first, pl.row_off, pl.esc_sorted, st);
+                } catch (...) {
+                    cudaStreamEndCapture(st, &graph);
+                    if (graph) cudaGraphDestroy(graph);
+                    throw;
+                }
+                PTC_CUDA(cudaStreamEndCapture(st, &graph));
+                const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+                if (ie != cudaSuccess) {
+                    cudaGraphDestroy(graph);
+                    throw Error{PTC_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ie)};
+                }
+            }
+            const cudaError_t le = work ? cudaGraphLaunch(exec, st) : cudaSuccess;
+            PTC_CUDA(cudaEventRecord(ev.ev[EV_WAVE1], st));
+            const cudaError_t se = cudaStreamSynchronize(st);
+            if (exec) cudaGraphExecDestroy(exec);
+            if (graph) cudaGraphDestroy(graph);
+            PTC_CUDA(le);
+            PTC_CUDA(se);
+            t_numeric += ev.ms(EV_WAVE0, EV_WAVE1);
+            PTC_REQUIRE(read_scalar(op.err, st) == 0, PTC_ERR_INTERNAL,
+                        "an accumulator table overflowed or met an out-of-range column");
+
+            // entries of each item; items with a failed claim or table are rerun exactly below
+            std::vector<uint64_t> nnz(S.begin() + i0, S.begin() + i1);
+            if (learned) {
+                const uint32_t nfail = read_scalar(ov.fail_count, st);
+                if (nfail > 0) {
+                    PartItem* fp = ar.alloc<PartItem>(nfail);
+                    launch_gather_parts(parts + pb[w], ov.fail_list, nfail, fp, st);
+                    std::vector<PartItem> hf(nfail);
+                    PTC_CUDA(cudaMemcpyAsync(hf.data(), fp, nfail * sizeof(PartItem), cudaMemcpyDeviceToHost, st));
+                    PTC_CUDA(cudaStreamSynchronize(st));
+                    for (const PartItem& p : hf) {
+                        const uint32_t it =
+                            (uint32_t)(std::upper_bound(rf.begin(), rf.end(), p.row) - rf.begin()) - 1;
+                        failed[it] = 1;
+                    }
+                }
+                std::vector<uint64_t> cur(i1 - i0), over(i1 - i0);
+                PTC_CUDA(cudaMemcpyAsync(cur.data(), ov.cursor + i0, (i1 - i0) * 8, cudaMemcpyDeviceToHost, st));
+                PTC_CUDA(cudaMemcpyAsync(over.data(), ov.overshoot + i0, (i1 - i0) * 8, cudaMemcpyDeviceToHost, st));
+                PTC_CUDA(cudaStreamSynchronize(st));
+                for (uint32_t i = i0; i < i1; ++i) nnz[i - i0] = cur[i - i0] - over[i - i0] - E[i];
+            }
+
+            // ---- hand the wave's outputs over ----
+            const auto t0 = std::chrono::steady_clock::now();
+            const void* src_idx = blk_idx;
+            const void* src_val = blk_val;
+            uint32_t loc = opt.output_location;
+            SharedBlock* shared = nullptr;
+            if (tg.outs) {
+                shared = new SharedBlock;
+                shared->location = loc;
+                if (loc == PTC_DEVICE) {
+                    shared->idx = blk_idx;
+                    shared->val = blk_val;
+                    blk_idx = nullptr;
+                    blk_val = nullptr;
+                } else {
+                    shared->idx = host_result_alloc(std::max<uint64_t>(wave_words[w], 1) * 4);
+                    shared->val = host_result_alloc(std::max<uint64_t>(wave_vals[w], 1) * 8);
+                    if (!shared->idx || !shared->val) {
+                        std::free(shared->idx);
+                        std::free(shared->val);
+                        delete shared;
+                        throw Error{PTC_ERR_OUT_OF_MEMORY, "host output allocation failed"};
+                    }
+                    host_copier().copy(shared->idx, blk_idx, wave_words[w] * 4, st);
+                    host_copier().copy(shared->val, blk_val, wave_vals[w] * 8, st);
+                }
+                src_idx = shared->idx;
+                src_val = shared->val;
+            } else if (host_view) {
+                host_copier().copy(host_blk_idx, blk_idx, wave_words[w] * 4, st);
+                host_copier().copy(host_blk_val, blk_val, wave_vals[w] * 8, st);
+                src_idx = host_blk_idx;
+                src_val = host_blk_val;
+            } else if (tg.sink) {
+                loc = PTC_DEVICE;  // device views of the reused block
+            }
+            uint32_t refs = 0;
+            for (uint32_t i = i0; i < i1; ++i) {
+                if (failed[i]) continue;
+                ptc_tensor t;
+                std::memset(&t, 0, sizeof(t));
+                t.order = items[i].fa + items[i].fb;
+                t.location = loc;
+                t.nnz = nnz[i - i0];
+                if (t.nnz > 0) {
+                    t.idx = const_cast<uint32_t*>(static_cast<const uint32_t*>(src_idx)) + io[i].idx0;
+                    t.vals = const_cast<double*>(static_cast<const double*>(src_val)) + io[i].val0;
+                }
+                stats.out_nnz += t.nnz;
+                if (tg.outs) {
+                    if (t.nnz > 0) {
+                        t.opaque = shared;
+                        ++refs;
+                    }
+                    tg.outs[tg.ids[i]] = t;
+                }
+                if (tg.sink) tg.sink(tg.user, tg.ids[i], &t);
+            }
+            if (shared) {
+                shared->refs = refs + 1;
+                release_block(shared);  // drops the wave's own reference
+            }
+            t_out += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        }
+    } catch (...) {
+        free_blocks();
+        throw;
+    }
+    free_blocks();
+    PTC_CUDA(cudaEventRecord(ev.ev[EV_D2H], st));
+    ar.release();
+    PTC_CUDA(cudaStreamSynchronize(st));
+    stats.t_h2d_ms += ev.ms(EV_START, EV_H2D);
+    stats.t_build_ms += ev.ms(EV_H2D, EV_ASIDE);
+    stats.t_symbolic_ms += ev.ms(EV_ASIDE, EV_SYM);
+    stats.t_numeric_ms += t_numeric;
+    stats.t_d2h_ms += t_out;
+    stats.t_total_ms += ev.ms(EV_START, EV_D2H);
+
+    // learned path: items whose prediction fell short run again, exactly
+    std::vector<BatchItemHost> again;
+    BatchTarget tg2;
+    tg2.outs = tg.outs;
+    tg2.sink = tg.sink;
+    tg2.user = tg.user;
+    for (uint32_t i = 0; i < n; ++i)
+        if (failed[i]) {
+            again.push_back(items[i]);
+            tg2.ids.push_back(tg.ids[i]);
+            stats.rerun_rows += rf[i + 1] - rf[i];
+        }
+    stats.rerun_items += again.size();
+    if (!again.empty()) {
+        ptc_stats s2;
+        std::memset(&s2, 0, sizeof(s2));
+        batch_impl(again, location, opt, true, tg2, s2);
+        stats.out_nnz += s2.out_nnz;
+        stats.t_total_ms += s2.t_total_ms;
+        stats.t_numeric_ms += s2.t_numeric_ms;
+    }
 }
 
 }  // namespace
@@ -891,9 +1708,78 @@ ptc_status ptc_self_contract(const uint32_t* hedges, const double* vals, uint32_
     return ptc_contract(&A, nullptr, c, dim_tc, dim_tc, opt, out, stats);
 }
 
+ptc_status ptc_batch_contract(const ptc_batch_item* items, uint32_t n, const ptc_options* opt_in, ptc_tensor* outs,
+                              ptc_batch_sink sink, void* user, ptc_stats* stats_out) {
+    using namespace ptc;
+    try {
+        PTC_REQUIRE(items != nullptr || n == 0, PTC_ERR_INVALID_ARGUMENT, "items is null");
+        const ptc_options opt = resolve_options(opt_in);
+        ptc_stats stats;
+        std::memset(&stats, 0, sizeof(stats));
+        g_launches = 0;
+        std::vector<BatchItemHost> hi(n);
+        uint32_t location = PTC_HOST;
+        for (uint32_t i = 0; i < n; ++i) {
+            const ptc_batch_item& it = items[i];
+            const bool self = it.B.idx == nullptr && it.B.nnz == 0 && it.B.dims == nullptr;
+            BatchItemHost& h = hi[i];
+            h.A = &it.A;
+            h.self = self;
+            h.B = self ? &it.A : &it.B;
+            h.c = it.c;
+            h.a_modes = it.a_modes;
+            h.b_modes = self ? it.a_modes : it.b_modes;
+            const std::string where = "item " + std::to_string(i) + ": ";
+            validate_pair(h.A, h.B, h.c, h.a_modes, h.b_modes, where);
+            h.fa = h.A->order - h.c;
+            h.fb = h.B->order - h.c;
+            if (i == 0) location = it.A.location;
+            PTC_REQUIRE(h.A->location == location && h.B->location == location, PTC_ERR_INVALID_ARGUMENT,
+                        where + "every input of a batch must be in the same memory");
+        }
+        BatchTarget tg;
+        tg.outs = outs;
+        tg.sink = sink;
+        tg.user = user;
+        tg.ids.resize(n);
+        for (uint32_t i = 0; i < n; ++i) {
+            tg.ids[i] = i;
+            if (outs) {
+                std::memset(&outs[i], 0, sizeof(ptc_tensor));
+                outs[i].order = hi[i].fa + hi[i].fb;
+                outs[i].location = opt.output_location;
+            }
+        }
+        if (n > 0) {
+            try {
+                batch_impl(hi, location, opt, false, tg, stats);
+            } catch (...) {
+                if (outs)
+                    for (uint32_t i = 0; i < n; ++i) ptc_tensor_free(&outs[i]);
+                throw;
+            }
+        }
+        stats.kernel_launches = g_launches;
+        if (stats_out) *stats_out = stats;
+        g_last_error.clear();
+        return PTC_OK;
+    } catch (const Error& e) {
+        set_last_error(e.status, e.msg);
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        set_last_error(PTC_ERR_OUT_OF_MEMORY, "host allocation failed");
+        return PTC_ERR_OUT_OF_MEMORY;
+    } catch (...) {
+        set_last_error(PTC_ERR_INTERNAL, "unexpected exception");
+        return PTC_ERR_INTERNAL;
+    }
+}
+
 void ptc_tensor_free(ptc_tensor* t) {
     if (!t) return;
-    if (t->location == PTC_DEVICE) {
+    if (t->opaque) {  // a slice of a batch wave's shared block
+        ptc::release_block(static_cast<ptc::SharedBlock*>(t->opaque));
+    } else if (t->location == PTC_DEVICE) {
         if (t->idx) cudaFree(t->idx);
         if (t->vals) cudaFree(t->vals);
     } else {
@@ -902,6 +1788,7 @@ void ptc_tensor_free(ptc_tensor* t) {
     }
     t->idx = nullptr;
     t->vals = nullptr;
+    t->opaque = nullptr;
     t->nnz = 0;
 }
 

@@ -71,20 +71,19 @@ __global__ void esc_gather_kernel(const double* __restrict__ val, const uint32_t
     if (i < n) sorted[i] = val[perm[i]];
 }
 
-// One thread per run: left fold of the run's products in stream order, written at the row's
+// One thread per run of [r0, r1): left fold of the run's products in stream order, written at the row's
 // output offset plus the run's rank inside the row.  Loads are issued eight at a time ahead of
 // the dependent additions.
 __global__ void esc_fold_kernel(Operands op, OutputView out, const uint64_t* __restrict__ run_key,
-                                const uint32_t* __restrict__ run_start, uint64_t nruns, uint32_t colbits,
+                                const uint32_t* __restrict__ run_start, uint64_t r0, uint64_t r1, uint32_t colbits,
                                 const uint32_t* __restrict__ esc_rows, const uint32_t* __restrict__ first_run,
                                 const uint64_t* __restrict__ row_off, const double* __restrict__ sorted) {
-    const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= nruns) return;
+    const uint64_t r = r0 + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= r1) return;
     const uint64_t key = run_key[r];
     const uint32_t e = (uint32_t)(key >> colbits);
     const uint32_t row = esc_rows[e];
-    uint32_t col = (uint32_t)(key & ((1ull << colbits) - 1));
-    if (op.row_colbase) col += op.row_colbase[row];  // item-local -> global column
+    const uint32_t col = (uint32_t)(key & ((1ull << colbits) - 1));
     const uint32_t b = run_start[r], en = run_start[r + 1];
     double v = sorted[b];
     uint32_t i = b + 1;
@@ -109,24 +108,22 @@ __global__ void esc_fold_kernel(Operands op, OutputView out, const uint64_t* __r
         for (uint32_t u = 0; u < U; ++u) v = __dadd_rn(v, cur[u]);
     }
     for (; i < en; ++i) v = __dadd_rn(v, sorted[i]);
-    const uint64_t o = row_off[row] + (r - first_run[e]);
-    const uint32_t fa = op.fa, fb = op.fb, od = fa + fb;
-    uint32_t* dst = out.idx + o * od;
-    for (uint32_t m = 0; m < fa; ++m) dst[m] = op.row_tuple[(uint64_t)row * fa + m];
-    for (uint32_t m = 0; m < fb; ++m) dst[fa + m] = op.col_tuple[(uint64_t)col * fb + m];
-    out.val[o] = v;
+    write_entry(op, out, row_off[row] + (r - first_run[e]), row, col, v);
 }
 
-void launch_esc_fold(const Operands& op, const OutputView& out, const uint64_t* run_key, const uint32_t* run_start,
-                     uint64_t nruns, uint32_t colbits, const uint32_t* esc_rows, const uint32_t* first_run,
-                     const uint64_t* row_off, const uint32_t* perm, const double* val, uint64_t nprod,
-                     double* sorted, cudaStream_t st) {
-    if (nruns == 0) return;
+void launch_esc_gather(const uint32_t* perm, const double* val, uint64_t nprod, double* sorted, cudaStream_t st) {
+    if (nprod == 0) return;
     esc_gather_kernel<<<ceil_div_u32(nprod, 256), 256, 0, st>>>(val, perm, nprod, sorted);
     count_launch();
     PTC_CHECK_LAUNCH();
-    esc_fold_kernel<<<ceil_div_u32(nruns, 128), 128, 0, st>>>(op, out, run_key, run_start, nruns, colbits, esc_rows,
-                                                             first_run, row_off, sorted);
+}
+
+void launch_esc_fold(const Operands& op, const OutputView& out, const uint64_t* run_key, const uint32_t* run_start,
+                     uint64_t r0, uint64_t r1, uint32_t colbits, const uint32_t* esc_rows, const uint32_t* first_run,
+                     const uint64_t* row_off, const double* sorted, cudaStream_t st) {
+    if (r1 <= r0) return;
+    esc_fold_kernel<<<ceil_div_u32(r1 - r0, 128), 128, 0, st>>>(op, out, run_key, run_start, r0, r1, colbits,
+                                                                esc_rows, first_run, row_off, sorted);
     count_launch();
     PTC_CHECK_LAUNCH();
 }

@@ -113,4 +113,64 @@ void launch_log2_error(const uint32_t* rows, uint64_t n, const float* pred, cons
     PTC_CHECK_LAUNCH();
 }
 
+// ---- claim budgets and batch waves ----
+
+// budget[rows[i]] = sum of the row's predicted panel counts (the budgets of its parts)
+__global__ void big_budget_kernel(const uint32_t* __restrict__ rows, uint64_t n, const uint32_t* __restrict__ cnt,
+                                  uint32_t P, uint64_t* __restrict__ budget) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint64_t s = 0;
+    for (uint32_t p = 0; p < P; ++p) s += cnt[i * P + p];
+    budget[rows[i]] = s;
+}
+
+void launch_claim_budgets(const uint32_t* big_rows, uint64_t n_big, const uint32_t* panel_cnt, uint32_t P,
+                          uint64_t* budget, cudaStream_t st) {
+    if (n_big == 0) return;
+    big_budget_kernel<<<ceil_div_u32(n_big, 256), 256, 0, st>>>(big_rows, n_big, panel_cnt, P, budget);
+    count_launch();
+    PTC_CHECK_LAUNCH();
+}
+
+// row_off[r] += claim_off[row_first[row_item[r]]] for every row r: the exactly counted entries of
+// an item go first in its range, ahead of the claimed ones
+__global__ void shift_exact_kernel(uint64_t nrows, const uint32_t* __restrict__ row_item,
+                                   const uint32_t* __restrict__ row_first, const uint64_t* __restrict__ claim_off,
+                                   uint64_t* __restrict__ row_off) {
+    const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < nrows) row_off[r] += claim_off[row_first[row_item[r]]];
+}
+
+void launch_shift_exact(uint64_t nrows, const uint32_t* row_item, const uint32_t* row_first, const uint64_t* claim_off,
+                        uint64_t* row_off, cudaStream_t st) {
+    if (nrows == 0) return;
+    shift_exact_kernel<<<ceil_div_u32(nrows, 256), 256, 0, st>>>(nrows, row_item, row_first, claim_off, row_off);
+    count_launch();
+    PTC_CHECK_LAUNCH();
+}
+
+// key[i] = wave of part i: the last wave whose first row is <= the part's row
+__global__ void part_wave_kernel(const PartItem* __restrict__ parts, uint32_t n, const uint32_t* __restrict__ wave_row,
+                                 uint32_t nwaves, uint64_t* __restrict__ key, uint32_t* __restrict__ idx) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t r = parts[i].row;
+    uint32_t lo = 0, hi = nwaves;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (wave_row[mid] <= r) lo = mid; else hi = mid;
+    }
+    key[i] = lo;
+    idx[i] = i;
+}
+
+void launch_part_wave(const PartItem* parts, uint32_t n, const uint32_t* wave_row, uint32_t nwaves, uint64_t* key,
+                      uint32_t* idx, cudaStream_t st) {
+    if (n == 0) return;
+    part_wave_kernel<<<ceil_div_u32(n, 256), 256, 0, st>>>(parts, n, wave_row, nwaves, key, idx);
+    count_launch();
+    PTC_CHECK_LAUNCH();
+}
+
 }  // namespace ptc

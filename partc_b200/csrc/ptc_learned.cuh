@@ -25,4 +25,14 @@ void launch_count_parts_range(const PartItem* parts, const uint32_t* ridx, uint3
 void launch_fill_parts_range(const PartItem* parts, const uint32_t* ridx, uint32_t n, const uint32_t* panel_cnt,
                              uint32_t P, SplitRule rule, const uint32_t* part_pos, PartItem* out, cudaStream_t st);
 
+// Claim budgets of the learned path: budget[big_rows[i]] = sum of the row's predicted panel counts.
+void launch_claim_budgets(const uint32_t* big_rows, uint64_t n_big, const uint32_t* panel_cnt, uint32_t P,
+                          uint64_t* budget, cudaStream_t st);
+// row_off[r] += claim_off[row_first[row_item[r]]] for every row
+void launch_shift_exact(uint64_t nrows, const uint32_t* row_item, const uint32_t* row_first, const uint64_t* claim_off,
+                        uint64_t* row_off, cudaStream_t st);
+// key[i] = wave of part i (waves start at rows wave_row[0..nwaves)), idx[i] = i
+void launch_part_wave(const PartItem* parts, uint32_t n, const uint32_t* wave_row, uint32_t nwaves, uint64_t* key,
+                      uint32_t* idx, cudaStream_t st);
+
 }  // namespace ptc

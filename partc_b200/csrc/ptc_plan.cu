@@ -150,7 +150,7 @@ __global__ void fill_parts_kernel(const uint32_t* __restrict__ rows, const uint3
         it.p0 = p0;
         it.p1 = p1;
         it.mode = mode;
-        it.out_off = row_off ? base + before : kClaimOffset;
+        it.out_off = row_off ? base + before : kClaimBit;
         parts[o++] = it;
     });
 }
@@ -201,7 +201,7 @@ __global__ void fill_parts_range_kernel(const PartItem* __restrict__ parts, cons
         x.p0 = it.p0 + q0;
         x.p1 = it.p0 + q1;
         x.mode = mode;
-        x.out_off = kClaimOffset;
+        x.out_off = kClaimBit;
         out[o++] = x;
     });
 }

@@ -37,28 +37,6 @@ __device__ __forceinline__ void accumulate(double* slot, double p) {
     *slot = (__double_as_longlong(v) == (long long)kNoValue) ? p : __dadd_rn(v, p);
 }
 
-// Write output entry o = (row's A free tuple, column's B free tuple, value); `col` is local to
-// the row's item.
-__device__ __forceinline__ void write_entry(const Operands& op, const OutputView& out, uint64_t o, uint32_t row,
-                                            uint32_t col, double v) {
-    if (op.row_colbase) col += op.row_colbase[row];
-    const uint32_t fa = op.fa, fb = op.fb, od = fa + fb;
-    uint32_t* dst = out.idx + o * od;
-    if (fa == 2 && fb == 2) {
-        const uint2 r = *reinterpret_cast<const uint2*>(op.row_tuple + (uint64_t)row * 2);
-        const uint2 c = *reinterpret_cast<const uint2*>(op.col_tuple + (uint64_t)col * 2);
-        *reinterpret_cast<uint4*>(dst) = make_uint4(r.x, r.y, c.x, c.y);
-    } else if (fa == 1 && fb == 1) {
-        *reinterpret_cast<uint2*>(dst) = make_uint2(op.row_tuple[row], op.col_tuple[col]);
-    } else {
-        for (uint32_t m = 0; m < fa; ++m) dst[m] = op.row_tuple[(uint64_t)row * fa + m];
-        for (uint32_t m = 0; m < fb; ++m) dst[fa + m] = op.col_tuple[(uint64_t)col * fb + m];
-    }
-    out.val[o] = v;
-}
-
-// Fiber entries of A nonzero k that fall in fine panels [p0, p1) (the whole fiber when the
-// column space is a single panel).
 // first entry of [lo, hi) (a fiber, sorted by column) whose column is >= c
 __device__ __forceinline__ uint32_t col_lower_bound(const uint32_t* __restrict__ col, uint32_t lo, uint32_t hi,
                                                    uint32_t c) {
@@ -69,6 +47,8 @@ __device__ __forceinline__ uint32_t col_lower_bound(const uint32_t* __restrict__
     return lo;
 }
 
+// Fiber entries [s, e) of fiber f whose columns fall in fine panels [p0, p1) (the whole fiber
+// when the column space is a single panel).
 __device__ __forceinline__ void part_range(const Operands& op, int32_t f, uint32_t p0, uint32_t p1, uint32_t& s,
                                            uint32_t& e) {
     if (op.panel_off) {
@@ -179,22 +159,8 @@ __global__ void __launch_bounds__(kSmallWarps * 32)
             }
         }
         // emit (numeric) or count (symbolic), resetting the table
-        uint64_t o = 0;
-        if (NUMERIC) {
-            if (row_off) {
-                o = row_off[row];
-            } else {  // claim mode: count first, then take a range at the output cursor
-                uint32_t cnt = 0;
-                for (uint32_t i = 0; i < kSmallSlots; i += 32)
-                    cnt += __popc(__ballot_sync(kFullMask, keys[i + lane] != kEmptyCol));
-                if (lane == 0) {
-                    o = claim_output(out, cnt);
-                    if (o == ~0ull) atomicOr(op.err, 2u);  // capacity is reserved for these rows
-                }
-                o = __shfl_sync(kFullMask, o, 0);
-            }
-        }
-        const bool write = NUMERIC && o != ~0ull;
+        uint64_t o = NUMERIC ? row_off[row] : 0;
+        const bool write = NUMERIC;
         for (uint32_t i = 0; i < kSmallSlots; i += 32) {
             const uint32_t sidx = i + lane;
             const uint32_t kc = keys[sidx];
@@ -571,8 +537,8 @@ __global__ void __launch_bounds__(kPartThreads, 2)
         if (t == 0) {
             uint64_t base = it.out_off, total = 0;
             for (uint32_t w = 0; w < kPartWarps; ++w) total += wtot[w];
-            if (base == kClaimOffset) {
-                base = any_bad ? ~0ull : claim_output(out, total);
+            if (base == kClaimBit) {
+                base = any_bad ? ~0ull : claim_output(op, out, row, total);
                 if (base == ~0ull) {  // rerun this part exactly
                     const uint32_t f = atomicAdd(out.fail_count, 1u);
                     out.fail_list[f] = item;

@@ -48,10 +48,12 @@ void launch_esc_expand(const Operands& op, const uint32_t* a_row, const int32_t*
                        cudaStream_t st);
 void launch_esc_count(const uint64_t* run_key, uint64_t nruns, uint32_t colbits, const uint32_t* esc_rows,
                       uint64_t* row_d, uint32_t* first_run, cudaStream_t st);
+// sorted[i] = val[perm[i]] for the nprod sorted products
+void launch_esc_gather(const uint32_t* perm, const double* val, uint64_t nprod, double* sorted, cudaStream_t st);
+// runs [r0, r1) of the sorted products: one output entry each
 void launch_esc_fold(const Operands& op, const OutputView& out, const uint64_t* run_key, const uint32_t* run_start,
-                     uint64_t nruns, uint32_t colbits, const uint32_t* esc_rows, const uint32_t* first_run,
-                     const uint64_t* row_off, const uint32_t* perm, const double* val, uint64_t nprod,
-                     double* sorted, cudaStream_t st);
+                     uint64_t r0, uint64_t r1, uint32_t colbits, const uint32_t* esc_rows, const uint32_t* first_run,
+                     const uint64_t* row_off, const double* sorted, cudaStream_t st);
 // out[pos[i]] = i wherever flag[i] (pos = exclusive scan of flag)
 void launch_compact_indices(const uint32_t* flag, const uint32_t* pos, uint64_t n, uint32_t* out, cudaStream_t st);
 // key[i] = ~row_flops[rows[i]] (descending-work sort key)
