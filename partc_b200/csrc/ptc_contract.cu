@@ -462,33 +462,44 @@ void grow_output(OutputView& ov, uint32_t od, uint64_t used, uint64_t need, cuda
     ov.capacity = need;
 }
 
-// Learned path of a single contraction, after the first numeric pass: parts whose accumulator
-// overflowed or whose claim did not fit wrote nothing and are listed in ov.fail_list.  Their rows
-// get the exact symbolic pass, each failed part is re-split exactly, and the new parts claim
-// after the entries already written (their sizes are exact, so they cannot fail again).  Returns
-// the output nnz.
-uint64_t learned_reruns(const Operands& op, const PartItem* parts, uint32_t n_parts, const uint32_t* big_rows,
-                        uint32_t n_big, const float* pred, const SplitRule& rule, OutputView& ov,
-                        uint32_t* work_counter, uint32_t* err, int num_sms, uint64_t nrows, Arena& ar,
-                        ptc_stats& stats) {
+// Work items of one launch on the learned path and what the launch reported about them.
+struct Launched {
+    int kind;                 // 0 warp tasks, 1 block parts
+    const PartItem* parts;
+    uint32_t n;
+    uint32_t* fail_list;
+    uint32_t* fail_count;
+    uint32_t* item_count;
+};
+
+// Learned path of a single contraction, after the first numeric pass: work items whose
+// accumulator overflowed or whose claim did not fit wrote nothing and are listed in their launch's
+// fail list.  Their rows get the exact symbolic pass, each failed item is re-split exactly into
+// block parts, and those claim after the entries already written (their sizes are exact, so they
+// cannot fail again).  Returns the output nnz.
+uint64_t learned_reruns(const Operands& op, std::vector<Launched> groups, const uint32_t* big_rows, uint32_t n_big,
+                        const float* pred, const SplitRule& rule, OutputView& ov, uint32_t* work_counter,
+                        uint32_t* err, int num_sms, uint64_t nrows, Arena& ar, ptc_stats& stats) {
     cudaStream_t st = ar.stream();
     const uint32_t P = op.npanels;
     uint64_t* row_actual = ar.alloc<uint64_t>(nrows);
     PTC_CUDA(cudaMemsetAsync(row_actual, 0, nrows * sizeof(uint64_t), st));
-    launch_row_actual(parts, ov.item_count, n_parts, row_actual, st);
-    const PartItem* cur = parts;
+    for (const Launched& g : groups) launch_row_actual(g.parts, g.item_count, g.n, row_actual, st);
     uint64_t rerun_rows = 0;
     for (int round = 0;; ++round) {
-        const uint32_t nfail = read_scalar(ov.fail_count, st);
+        std::vector<uint32_t> nf(groups.size());
+        uint32_t nfail = 0;
+        for (size_t gi = 0; gi < groups.size(); ++gi) nfail += (nf[gi] = read_scalar(groups[gi].fail_count, st));
         if (nfail == 0) break;
         PTC_REQUIRE(round < 4, PTC_ERR_INTERNAL, "exactly sized parts failed again");
         PartItem* failed = ar.alloc<PartItem>(nfail);
-        launch_gather_parts(cur, ov.fail_list, nfail, failed, st);
+        for (size_t gi = 0, at = 0; gi < groups.size(); at += nf[gi], ++gi)
+            launch_gather_parts(groups[gi].parts, groups[gi].fail_list, nf[gi], failed + at, st);
         std::vector<PartItem> hf(nfail);
         PTC_CUDA(cudaMemcpyAsync(hf.data(), failed, nfail * sizeof(PartItem), cudaMemcpyDeviceToHost, st));
         PTC_CUDA(cudaStreamSynchronize(st));
         std::vector<uint32_t> hrows, hridx(nfail);
-        for (uint32_t i = 0; i < nfail; ++i) {  // failed parts are few
+        for (uint32_t i = 0; i < nfail; ++i) {  // failed items are few
             uint32_t r = 0;
             while (r < hrows.size() && hrows[r] != hf[i].row) ++r;
             if (r == hrows.size()) hrows.push_back(hf[i].row);
@@ -519,12 +530,16 @@ uint64_t learned_reruns(const Operands& op, const PartItem* parts, uint32_t n_pa
         PTC_CUDA(cudaMemsetAsync(ov.overshoot, 0, sizeof(uint64_t), st));
         PartItem* fresh = ar.alloc<PartItem>(nnew);
         launch_fill_parts_range(failed, dridx, nfail, cnt, P, rule, np, fresh, st);
-        ov.fail_list = ar.alloc<uint32_t>(std::max<uint32_t>(nnew, 1));
-        ov.item_count = ar.alloc<uint32_t>(std::max<uint32_t>(nnew, 1));
-        PTC_CUDA(cudaMemsetAsync(ov.fail_count, 0, sizeof(uint32_t), st));
-        launch_hash_parts(op, fresh, nnew, ov, work_counter, err, num_sms, st);
-        launch_row_actual(fresh, ov.item_count, nnew, row_actual, st);
-        cur = fresh;
+        Launched g{1, fresh, nnew, ar.alloc<uint32_t>(std::max<uint32_t>(nnew, 1)), groups[0].fail_count,
+                   ar.alloc<uint32_t>(std::max<uint32_t>(nnew, 1))};
+        for (const Launched& old : groups) PTC_CUDA(cudaMemsetAsync(old.fail_count, 0, sizeof(uint32_t), st));
+        OutputView o2 = ov;
+        o2.fail_list = g.fail_list;
+        o2.fail_count = g.fail_count;
+        o2.item_count = g.item_count;
+        launch_hash_parts(op, fresh, nnew, o2, work_counter, err, num_sms, st);
+        launch_row_actual(fresh, g.item_count, nnew, row_actual, st);
+        groups.assign(1, g);
     }
     stats.rerun_rows = rerun_rows;
     double* esum = ar.alloc<double>(1);
@@ -595,12 +610,22 @@ struct Plan {
     uint64_t* claim_off = nullptr;
     uint64_t exact_nnz = 0, claim_total = 0;
     float* pred = nullptr;
-    SplitRule rule{};
-    PartItem* parts = nullptr;
-    uint32_t n_parts = 0;
+    // work items of the large rows: [0] warp tasks (rows with at most kWarpTaskMaxLen A nonzeros,
+    // big_rows[0, n_warp_rows)), [1] block parts (the others)
+    uint32_t n_warp_rows = 0;
+    SplitRule rule[2]{};
+    PartItem* parts[2] = {nullptr, nullptr};
+    uint32_t n_parts[2] = {0, 0};
     uint32_t* work_counter = nullptr;
     bool collected = false;
 };
+
+// One kind of work item and its accumulator kernel.
+void launch_parts(int kind, const Operands& op, const PartItem* parts, uint32_t n, const OutputView& out,
+                  uint32_t* work_counter, uint32_t* err, int num_sms, cudaStream_t st) {
+    if (kind == 0) launch_warp_tasks(op, parts, n, out, work_counter, err, num_sms, st);
+    else launch_hash_parts(op, parts, n, out, work_counter, err, num_sms, st);
+}
 
 Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect* collect, int num_sms, Arena& ar,
                ptc_stats& stats) {
@@ -622,35 +647,6 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
     stats.nrows = nrows;
     stats.nfibers = nfib;
     if (pl.flops == 0) return pl;
-
-    // fine column panels: B fibers are split at multiples of W so a row can be cut into parts
-    // that each fit one shared-memory table (W <= table capacity, so a part always fits).  The
-    // per-fiber panel table is kept within 1 GiB (wider panels, else binary searches in the fiber).
-    PTC_REQUIRE(ncols <= sym_bitmap_max_cols(), PTC_ERR_INVALID_ARGUMENT,
-                "more than 1.5M distinct B free keys in one contraction is not supported yet");
-    auto table_bytes = [&](uint32_t w) { return nfib * ((ncols + w - 1) / w + 1) * 4; };
-    uint32_t W = opt.panel_width;
-    if (W == 0) {
-        W = 32;
-        while (W < 2048 && (uint64_t)W * 16 < ncols) W <<= 1;
-        uint32_t w2 = W;
-        while (w2 < 4096 && table_bytes(w2) > (1ull << 30)) w2 <<= 1;
-        if (table_bytes(w2) <= (1ull << 30)) W = w2;
-    }
-    PTC_REQUIRE(W <= hash_part_capacity(), PTC_ERR_INVALID_ARGUMENT, "panel_width larger than a hash part");
-    pl.W = W;
-    pl.log2w = floor_log2(W);
-    pl.P = (uint32_t)std::max<uint64_t>(1, (ncols + W - 1) / W);
-    const uint32_t P = pl.P;
-    stats.panel_width = W;
-    uint32_t* panel_off = nullptr;
-    if (P > 1 && table_bytes(W) <= (1ull << 30)) {
-        panel_off = ar.alloc<uint32_t>(nfib * (uint64_t)(P + 1));
-        launch_panel_offsets(op.b_col, F.b_fib, op.fib_start, nb, P, pl.log2w, panel_off, st);
-    }
-    op.panel_off = panel_off;
-    op.npanels = P;
-    op.panel_log2 = pl.log2w;
 
     // row classes and work lists (largest rows first)
     uint32_t* small_flag = ar.alloc<uint32_t>(nrows + 1);
@@ -689,19 +685,67 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
     launch_compact_indices(small_flag, pl.small_pos, nrows, pl.small_rows, st);
     launch_compact_indices(big_flag, big_pos, nrows, pl.big_rows, st);
     const uint32_t n_small = pl.n_small, n_big = pl.n_big, n_esc = pl.n_esc;
-    if (n_big > 1) {
+    // large rows: warp tasks for rows of at most kWarpTaskMaxLen A nonzeros (panels of at most
+    // a dense warp task's width), block parts for the others; each group largest first
+    const uint32_t warp_len = (opt.panel_width == 0 || opt.panel_width <= warp_task_dense_columns())
+                                  ? kWarpTaskMaxLen : 0u;
+    if (n_big > 0) {
         uint64_t* wkey = ar.alloc<uint64_t>(n_big);
-        launch_work_keys(pl.big_rows, n_big, pl.row_flops, wkey, st);
-        radix_sort_pairs(wkey, pl.big_rows, n_big, 0, 40, ar);
+        launch_work_keys(pl.big_rows, n_big, pl.row_flops, op.row_start, warp_len, wkey, st);
+        if (n_big > 1) radix_sort_pairs(wkey, pl.big_rows, n_big, 0, 41, ar);
+        const uint64_t split = 1ull << 40;
+        uint64_t* split_d = ar.alloc<uint64_t>(1);
+        uint32_t* first = ar.alloc<uint32_t>(2);
+        PTC_CUDA(cudaMemcpyAsync(split_d, &split, sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+        launch_key_bounds(wkey, n_big, split_d, 1, first, st);
+        pl.n_warp_rows = read_scalar(first, st);
     }
     stats.rows_small = n_small;
     stats.rows_hash = n_big;
     stats.rows_long = n_esc;
 
-    pl.rule.cap = hash_part_capacity();
-    pl.rule.dense_panels = dense_part_columns() >> pl.log2w;
-    pl.rule.dense_min = W / kDenseMinFraction;
-    pl.rule.min_bits = hash_part_min_bits();
+    // fine column panels: B fibers are split at multiples of W so a row can be cut into parts
+    // that each fit one shared-memory table (W <= table capacity, so a part always fits).  The
+    // per-fiber panel table is kept within 1 GiB (wider panels, else binary searches in the fiber).
+    PTC_REQUIRE(ncols <= sym_bitmap_max_cols(), PTC_ERR_INVALID_ARGUMENT,
+                "more than 1.5M distinct B free keys in one contraction is not supported yet");
+    auto table_bytes = [&](uint32_t w) { return nfib * ((ncols + w - 1) / w + 1) * 4; };
+    uint32_t W = opt.panel_width;
+    if (W == 0) {  // at most 256 columns (a quarter of a dense warp task), wider for small tables
+        W = 32;
+        while (W < 256 && (uint64_t)W * 16 < ncols) W <<= 1;
+        while (W < warp_task_dense_columns() && (uint64_t)n_big * ((ncols + W - 1) / W) * 4 > (2ull << 30)) W <<= 1;
+    }
+    PTC_REQUIRE(W <= hash_part_capacity(), PTC_ERR_INVALID_ARGUMENT, "panel_width larger than a hash part");
+    pl.W = W;
+    pl.log2w = floor_log2(W);
+    pl.P = (uint32_t)std::max<uint64_t>(1, (ncols + W - 1) / W);
+    const uint32_t P = pl.P;
+    stats.panel_width = W;
+    uint32_t* panel_off = nullptr;
+    if (P > 1 && table_bytes(W) <= (1ull << 30)) {
+        panel_off = ar.alloc<uint32_t>(nfib * (uint64_t)(P + 1));
+        launch_panel_offsets(op.b_col, F.b_fib, op.fib_start, nb, P, pl.log2w, panel_off, st);
+    }
+    op.panel_off = panel_off;
+    op.npanels = P;
+    op.panel_log2 = pl.log2w;
+
+
+    SplitRule& wr = pl.rule[0];  // warp tasks
+    wr.cap = warp_task_capacity();
+    wr.dense_panels = warp_task_dense_columns() >> pl.log2w;
+    wr.dense_min = std::max(1u, W / 6);
+    wr.min_bits = warp_task_min_bits();
+    wr.max_bits = warp_task_max_bits();
+    wr.oversize_dense = 1;
+    SplitRule& br = pl.rule[1];  // block parts
+    br.cap = hash_part_capacity();
+    br.dense_panels = dense_part_columns() >> pl.log2w;
+    br.dense_min = W / kDenseMinFraction;
+    br.min_bits = hash_part_min_bits();
+    br.max_bits = 13;
+    br.oversize_dense = 0;
 
     // symbolic: exact output nnz of the small rows (both paths) and of the large rows (per fine
     // panel; two-phase path only -- the learned path predicts those)
@@ -774,16 +818,19 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
         pl.claim_total = read_scalar(pl.claim_off + nrows, st);
     }
 
-    // split large rows into parts that fit a shared-memory table
-    uint32_t* nparts = ar.alloc<uint32_t>((uint64_t)n_big + 1);
-    launch_count_parts(panel_cnt, n_big, P, pl.rule, nparts, op.err, st);
-    exclusive_scan<uint32_t>(nparts, nparts, n_big, ar);
-    pl.n_parts = read_scalar(nparts + n_big, st);
-    PTC_REQUIRE(read_scalar(op.err, st) == 0, PTC_ERR_INTERNAL, "a fine panel exceeds the hash part capacity");
-    pl.parts = ar.alloc<PartItem>(pl.n_parts);
-    launch_fill_parts(pl.big_rows, panel_cnt, n_big, P, pl.rule, nparts, pl.learned ? nullptr : pl.row_off, pl.parts,
-                      st);
-    stats.hash_parts = pl.n_parts;
+    // split large rows into tasks / parts that fit a shared-memory table
+    for (int kind = 0; kind < 2; ++kind) {
+        const uint64_t r0 = kind == 0 ? 0 : pl.n_warp_rows, nr = kind == 0 ? pl.n_warp_rows : n_big - pl.n_warp_rows;
+        uint32_t* nparts = ar.alloc<uint32_t>(nr + 1);
+        launch_count_parts(panel_cnt + r0 * P, nr, P, pl.rule[kind], nparts, op.err, st);
+        exclusive_scan<uint32_t>(nparts, nparts, nr, ar);
+        pl.n_parts[kind] = read_scalar(nparts + nr, st);
+        PTC_REQUIRE(read_scalar(op.err, st) == 0, PTC_ERR_INTERNAL, "a fine panel exceeds the hash part capacity");
+        pl.parts[kind] = ar.alloc<PartItem>(pl.n_parts[kind]);
+        launch_fill_parts(pl.big_rows + r0, panel_cnt + r0 * P, nr, P, pl.rule[kind], nparts,
+                          pl.learned ? nullptr : pl.row_off, pl.parts[kind], st);
+    }
+    stats.hash_parts = pl.n_parts[0] + pl.n_parts[1];
     return pl;
 }
 
@@ -930,20 +977,28 @@ void contract_impl(const ptc_coo* A, const ptc_coo* Bin, uint32_t c, const uint3
             ov.capacity = capacity;
             ov.cursor = ar.alloc<uint64_t>(1);
             ov.overshoot = ar.alloc<uint64_t>(1);
-            ov.fail_count = ar.alloc<uint32_t>(1);
-            ov.fail_list = ar.alloc<uint32_t>(std::max<uint32_t>(pl.n_parts, 1));
-            ov.item_count = ar.alloc<uint32_t>(std::max<uint32_t>(pl.n_parts, 1));
             PTC_CUDA(cudaMemcpyAsync(ov.cursor, &pl.exact_nnz, sizeof(uint64_t), cudaMemcpyHostToDevice, st));
             PTC_CUDA(cudaMemsetAsync(ov.overshoot, 0, sizeof(uint64_t), st));
-            PTC_CUDA(cudaMemsetAsync(ov.fail_count, 0, sizeof(uint32_t), st));
         }
+        std::vector<Launched> groups;
         launch_small_rows(true, op, pl.small_rows, pl.n_small, nullptr, pl.row_off, ov, st);
-        launch_hash_parts(op, pl.parts, pl.n_parts, ov, pl.work_counter, op.err, dev.num_sms, st);
+        for (int kind = 0; kind < 2; ++kind) {
+            OutputView o = ov;
+            if (learned) {
+                const uint32_t n = std::max<uint32_t>(pl.n_parts[kind], 1);
+                o.fail_count = ar.alloc<uint32_t>(1);
+                o.fail_list = ar.alloc<uint32_t>(n);
+                o.item_count = ar.alloc<uint32_t>(n);
+                PTC_CUDA(cudaMemsetAsync(o.fail_count, 0, sizeof(uint32_t), st));
+                groups.push_back({kind, pl.parts[kind], pl.n_parts[kind], o.fail_list, o.fail_count, o.item_count});
+            }
+            launch_parts(kind, op, pl.parts[kind], pl.n_parts[kind], o, pl.work_counter, op.err, dev.num_sms, st);
+        }
         launch_esc_fold(op, ov, pl.esc_run_key, pl.esc_run_start, 0, pl.esc_runs, pl.esc_colbits, pl.esc_rows,
                         pl.esc_first, pl.row_off, pl.esc_sorted, st);
         if (learned) {
-            out_nnz = learned_reruns(op, pl.parts, pl.n_parts, pl.big_rows, pl.n_big, pl.pred, pl.rule, ov,
-                                     pl.work_counter, op.err, dev.num_sms, op.nrows, ar, stats);
+            out_nnz = learned_reruns(op, groups, pl.big_rows, pl.n_big, pl.pred, pl.rule[1], ov, pl.work_counter,
+                                     op.err, dev.num_sms, op.nrows, ar, stats);
         }
         PTC_CUDA(cudaEventRecord(ev.ev[EV_NUM], st));
         PTC_REQUIRE(read_scalar(op.err, st) == 0, PTC_ERR_INTERNAL,
@@ -1343,25 +1398,28 @@ void batch_impl(const std::vector<BatchItemHost>& items, uint32_t location, cons
     // work of each wave: parts sorted by wave (largest first inside a wave), small rows, runs
     std::vector<uint32_t> wave_row(nw + 1);
     for (uint32_t w = 0; w <= nw; ++w) wave_row[w] = rf[wave_item[w]];
-    std::vector<uint32_t> pb(nw + 1, 0);
-    pb[nw] = pl.n_parts;
-    PartItem* parts = pl.parts;
-    if (nw > 1 && pl.n_parts > 0) {
-        uint32_t* wave_row_d = ar.alloc<uint32_t>(nw + 1);
-        PTC_CUDA(cudaMemcpyAsync(wave_row_d, wave_row.data(), (nw + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-        uint64_t* key = ar.alloc<uint64_t>(pl.n_parts);
-        uint32_t* idx = ar.alloc<uint32_t>(pl.n_parts);
-        launch_part_wave(pl.parts, pl.n_parts, wave_row_d, nw, key, idx, st);
-        radix_sort_pairs(key, idx, pl.n_parts, 0, bits_for_space(nw), ar);
-        parts = ar.alloc<PartItem>(pl.n_parts);
-        launch_gather_parts(pl.parts, idx, pl.n_parts, parts, st);
-        std::vector<uint64_t> wid(nw);
-        for (uint32_t w = 0; w < nw; ++w) wid[w] = w;
-        uint64_t* wid_d = ar.alloc<uint64_t>(nw);
-        PTC_CUDA(cudaMemcpyAsync(wid_d, wid.data(), nw * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+    std::vector<uint32_t> pb[2];
+    PartItem* parts[2] = {pl.parts[0], pl.parts[1]};
+    uint32_t* wave_row_d = ar.alloc<uint32_t>(nw + 1);
+    PTC_CUDA(cudaMemcpyAsync(wave_row_d, wave_row.data(), (nw + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    std::vector<uint64_t> wid(nw);
+    for (uint32_t w = 0; w < nw; ++w) wid[w] = w;
+    uint64_t* wid_d = ar.alloc<uint64_t>(nw);
+    PTC_CUDA(cudaMemcpyAsync(wid_d, wid.data(), nw * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+    for (int kind = 0; kind < 2; ++kind) {
+        const uint32_t np = pl.n_parts[kind];
+        pb[kind].assign(nw + 1, 0);
+        pb[kind][nw] = np;
+        if (nw == 1 || np == 0) continue;
+        uint64_t* key = ar.alloc<uint64_t>(np);
+        uint32_t* idx = ar.alloc<uint32_t>(np);
+        launch_part_wave(pl.parts[kind], np, wave_row_d, nw, key, idx, st);
+        radix_sort_pairs(key, idx, np, 0, bits_for_space(nw), ar);
+        parts[kind] = ar.alloc<PartItem>(np);
+        launch_gather_parts(pl.parts[kind], idx, np, parts[kind], st);
         uint32_t* bounds = ar.alloc<uint32_t>(nw + 1);
-        launch_key_bounds(key, pl.n_parts, wid_d, nw, bounds, st);
-        PTC_CUDA(cudaMemcpyAsync(pb.data(), bounds, (nw + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        launch_key_bounds(key, np, wid_d, nw, bounds, st);
+        PTC_CUDA(cudaMemcpyAsync(pb[kind].data(), bounds, (nw + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         PTC_CUDA(cudaStreamSynchronize(st));
     }
     const std::vector<uint32_t> sb = read_at<uint32_t>(pl.small_pos, wave_row, ar);
@@ -1383,10 +1441,15 @@ void batch_impl(const std::vector<BatchItemHost>& items, uint32_t location, cons
         PTC_CUDA(cudaMemcpyAsync(end_d, end.data(), n * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
         PTC_CUDA(cudaMemsetAsync(base.overshoot, 0, n * sizeof(uint64_t), st));
         base.cap_end = end_d;
-        base.fail_count = ar.alloc<uint32_t>(1);
-        base.fail_list = ar.alloc<uint32_t>(std::max<uint32_t>(pl.n_parts, 1));
         PTC_CUDA(cudaStreamSynchronize(st));  // the host vectors above go out of scope
     }
+    uint32_t* fail_count[2] = {nullptr, nullptr};
+    uint32_t* fail_list[2] = {nullptr, nullptr};
+    if (learned)
+        for (int kind = 0; kind < 2; ++kind) {
+            fail_count[kind] = ar.alloc<uint32_t>(1);
+            fail_list[kind] = ar.alloc<uint32_t>(std::max<uint32_t>(pl.n_parts[kind], 1));
+        }
 
     // output blocks: one per wave when the outputs are kept on the device, else one reused block
     uint64_t max_vals = 0, max_words = 0;
@@ -1448,9 +1511,16 @@ void batch_impl(const std::vector<BatchItemHost>& items, uint32_t location, cons
             OutputView ov = base;
             ov.idx = blk_idx;
             ov.val = blk_val;
-            if (learned) PTC_CUDA(cudaMemsetAsync(ov.fail_count, 0, sizeof(uint32_t), st));
+            OutputView ovk[2] = {ov, ov};
+            if (learned)
+                for (int kind = 0; kind < 2; ++kind) {
+                    ovk[kind].fail_count = fail_count[kind];
+                    ovk[kind].fail_list = fail_list[kind];
+                    PTC_CUDA(cudaMemsetAsync(fail_count[kind], 0, sizeof(uint32_t), st));
+                }
             PTC_CUDA(cudaEventRecord(ev.ev[EV_WAVE0], st));
-            const bool work = sb[w + 1] > sb[w] || pb[w + 1] > pb[w] || rb[w + 1] > rb[w];
+            const bool work = sb[w + 1] > sb[w] || pb[0][w + 1] > pb[0][w] || pb[1][w + 1] > pb[1][w] ||
+                              rb[w + 1] > rb[w];
             // the wave's numeric pass, captured and launched as one graph
             cudaGraph_t graph = nullptr;
             cudaGraphExec_t exec = nullptr;
@@ -1459,8 +1529,9 @@ void batch_impl(const std::vector<BatchItemHost>& items, uint32_t location, cons
                 try {
                     launch_small_rows(true, op, pl.small_rows + sb[w], sb[w + 1] - sb[w], nullptr, pl.row_off, ov,
                                       st);
-                    launch_hash_parts(op, parts + pb[w], pb[w + 1] - pb[w], ov, pl.work_counter, op.err, dev.num_sms,
-                                      st);
+                    for (int kind = 0; kind < 2; ++kind)
+                        launch_parts(kind, op, parts[kind] + pb[kind][w], pb[kind][w + 1] - pb[kind][w], ovk[kind],
+                                     pl.work_counter, op.err, dev.num_sms, st);
                     launch_esc_fold(op, ov, pl.esc_run_key, pl.esc_run_start, rb[w], rb[w + 1], pl.esc_colbits,
                                     pl.esc_rows, pl.esc_first, pl.row_off, pl.esc_sorted, st);
                 } catch (...) {
@@ -1489,17 +1560,19 @@ void batch_impl(const std::vector<BatchItemHost>& items, uint32_t location, cons
             // entries of each item; items with a failed claim or table are rerun exactly below
             std::vector<uint64_t> nnz(S.begin() + i0, S.begin() + i1);
             if (learned) {
-                const uint32_t nfail = read_scalar(ov.fail_count, st);
-                if (nfail > 0) {
-                    PartItem* fp = ar.alloc<PartItem>(nfail);
-                    launch_gather_parts(parts + pb[w], ov.fail_list, nfail, fp, st);
-                    std::vector<PartItem> hf(nfail);
-                    PTC_CUDA(cudaMemcpyAsync(hf.data(), fp, nfail * sizeof(PartItem), cudaMemcpyDeviceToHost, st));
-                    PTC_CUDA(cudaStreamSynchronize(st));
-                    for (const PartItem& p : hf) {
-                        const uint32_t it =
-                            (uint32_t)(std::upper_bound(rf.begin(), rf.end(), p.row) - rf.begin()) - 1;
-                        failed[it] = 1;
+                for (int kind = 0; kind < 2; ++kind) {
+                    const uint32_t nfail = read_scalar(fail_count[kind], st);
+                    if (nfail > 0) {
+                        PartItem* fp = ar.alloc<PartItem>(nfail);
+                        launch_gather_parts(parts[kind] + pb[kind][w], fail_list[kind], nfail, fp, st);
+                        std::vector<PartItem> hf(nfail);
+                        PTC_CUDA(cudaMemcpyAsync(hf.data(), fp, nfail * sizeof(PartItem), cudaMemcpyDeviceToHost, st));
+                        PTC_CUDA(cudaStreamSynchronize(st));
+                        for (const PartItem& p : hf) {
+                            const uint32_t it =
+                                (uint32_t)(std::upper_bound(rf.begin(), rf.end(), p.row) - rf.begin()) - 1;
+                            failed[it] = 1;
+                        }
                     }
                 }
                 std::vector<uint64_t> cur(i1 - i0), over(i1 - i0);

@@ -55,14 +55,18 @@ void launch_compact_indices(const uint32_t* flag, const uint32_t* pos, uint64_t 
 }
 
 __global__ void work_keys_kernel(const uint32_t* __restrict__ rows, uint64_t n, const uint64_t* __restrict__ row_flops,
-                                 uint64_t* __restrict__ key) {
+                                 const uint32_t* __restrict__ row_start, uint32_t max_len, uint64_t* __restrict__ key) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) key[i] = ~row_flops[rows[i]];
+    if (i >= n) return;
+    const uint32_t r = rows[i];
+    const uint64_t block_row = (row_start[r + 1] - row_start[r]) > max_len ? 1ull : 0ull;
+    key[i] = (block_row << 40) | (~row_flops[r] & ((1ull << 40) - 1));
 }
 
-void launch_work_keys(const uint32_t* rows, uint64_t n, const uint64_t* row_flops, uint64_t* key, cudaStream_t st) {
+void launch_work_keys(const uint32_t* rows, uint64_t n, const uint64_t* row_flops, const uint32_t* row_start,
+                      uint32_t max_len, uint64_t* key, cudaStream_t st) {
     if (n == 0) return;
-    work_keys_kernel<<<ceil_div_u32(n, 256), 256, 0, st>>>(rows, n, row_flops, key);
+    work_keys_kernel<<<ceil_div_u32(n, 256), 256, 0, st>>>(rows, n, row_flops, row_start, max_len, key);
     count_launch();
     PTC_CHECK_LAUNCH();
 }
@@ -99,17 +103,23 @@ __device__ __forceinline__ uint32_t split_panels(const uint32_t* cnt, uint32_t P
         const uint32_t p0 = p;
         uint64_t acc = 0;
         while (p < P && (acc == 0 || acc + cnt[p] <= rule.cap)) {
-            if (cnt[p] > rule.cap) *oversize = true;
+            if (cnt[p] > rule.cap && !rule.oversize_dense) *oversize = true;
             acc += cnt[p];
             ++p;
             uint32_t w2;
             uint64_t s2;
             if (p < P && dense_window(p, w2, s2)) break;
         }
-        if (acc > 0) {
+        if (acc > rule.cap && rule.oversize_dense) {
+            // one panel above the table's capacity (the last one taken; those before it are
+            // empty): direct-mapped over that panel alone
+            emit(p - 1, p, before, 1u);
+            ++parts;
+            before += acc;
+        } else if (acc > 0) {
             // table of at least acc / 0.75 slots, a power of two
             uint32_t bits = rule.min_bits;
-            while (bits < 13 && ((uint64_t)3 << bits) < acc * 4) ++bits;
+            while (bits < rule.max_bits && ((uint64_t)3 << bits) < acc * 4) ++bits;
             emit(p0, p, before, bits << 1);
             ++parts;
             before += acc;

@@ -297,6 +297,196 @@ void launch_sym_bitmap(const Operands& op, const uint32_t* rows, uint32_t nrows,
 }
 
 // ---------------------------------------------------------------------------------------------
+// numeric pass, warp tasks: one warp per task -- a row's columns in fine panels [p0, p1) -- with
+// a private table in shared memory (dense: direct-mapped by column over at most kTaskDense
+// columns; sparse: open addressing, at most kTaskSlots slots).  Warps take tasks one at a time
+// from a counter, with no block-wide barrier.
+//
+// A task walks the row's A nonzeros 32 at a time: lane j finds its nonzero's fiber entries in the
+// task's panels, a warp scan packs those products into chunks of 32 in stream order, and every
+// lane takes one product of a chunk.  Inside a chunk, products of one column are applied in lane
+// order (= stream order) by rank (match_any); chunks run in order.  So every output value is the
+// left fold of its products in stream order, as in the reference.
+// ---------------------------------------------------------------------------------------------
+
+constexpr int kTaskWarps = 4;                               // warps per block
+constexpr uint32_t kTaskDense = 1024;                       // columns of a dense task
+constexpr uint32_t kTaskSlots = 512;                        // largest sparse table
+constexpr size_t kTaskBytes = kTaskDense * sizeof(double);  // shared memory per warp
+// the sparse layout keeps values in vals[0, 512) and keys in the bytes of vals[512, 768)
+static_assert(kTaskSlots * (sizeof(double) + sizeof(uint32_t)) <= kTaskBytes, "sparse layout fits a warp's region");
+
+uint32_t warp_task_capacity() { return kTaskSlots * 3 / 4; }  // load factor <= 0.75
+uint32_t warp_task_dense_columns() { return kTaskDense; }
+uint32_t warp_task_min_bits() { return 6; }                   // 64 slots: two per lane
+uint32_t warp_task_max_bits() { return 9; }
+
+__global__ void __launch_bounds__(kTaskWarps * 32, 6)
+    warp_task_kernel(Operands op, const PartItem* __restrict__ tasks, uint32_t ntasks, OutputView out,
+                     uint32_t* __restrict__ work_counter, uint32_t* __restrict__ overflow) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const uint32_t warp = threadIdx.x >> 5, lane = lane_id();
+    double* vals = reinterpret_cast<double*>(smem + warp * kTaskBytes);
+    unsigned long long* vbits = reinterpret_cast<unsigned long long*>(vals);
+    uint32_t* keys = reinterpret_cast<uint32_t*>(vals + kTaskSlots);
+    for (uint32_t i = lane; i < kTaskDense; i += 32) vbits[i] = kNoValue;
+    bool dense_layout = true;
+    __syncwarp();
+
+    for (;;) {
+        uint32_t t = 0;
+        if (lane == 0) t = atomicAdd(work_counter, 1u);
+        t = __shfl_sync(kFullMask, t, 0);
+        if (t >= ntasks) break;
+        const PartItem it = tasks[t];
+        const bool dense = (it.mode & 1u) != 0;
+        const uint32_t tsize = dense ? kTaskDense : (1u << (it.mode >> 1));
+        const uint32_t tmask = tsize - 1;
+        if (dense != dense_layout) {  // values are all empty after an emission; only keys differ
+            if (dense) {
+                for (uint32_t i = kTaskSlots + lane; i < kTaskSlots + kTaskSlots / 2; i += 32) vbits[i] = kNoValue;
+            } else {
+                for (uint32_t i = lane; i < kTaskSlots; i += 32) keys[i] = kEmptyCol;
+            }
+            dense_layout = dense;
+            __syncwarp();
+        }
+        const uint32_t row = it.row;
+        const uint32_t c0 = it.p0 << op.panel_log2;  // first column of the task
+        const uint32_t ka = op.row_start[row], kb = op.row_start[row + 1];
+        bool bad = false;  // table overflow or a column outside a dense task (never for exact sizes)
+
+        for (uint32_t kw = ka; kw < kb; kw += 32) {
+            const uint32_t k = kw + lane;
+            uint32_t L = 0, s = 0;
+            double a = 0.0;
+            if (k < kb) {
+                const int32_t f = op.a_fib[k];
+                if (f >= 0) {
+                    uint32_t e;
+                    part_range(op, f, it.p0, it.p1, s, e);
+                    L = e - s;
+                    a = op.a_val[k];
+                }
+            }
+            const uint32_t incl = warp_inclusive_scan(L);
+            const uint32_t excl = incl - L;
+            const uint32_t total = __shfl_sync(kFullMask, incl, 31);
+            for (uint32_t q0 = 0; q0 < total; q0 += 32) {
+                const uint32_t q = q0 + lane;
+                const bool valid = q < total;
+                // source lane: number of lanes whose inclusive end is <= q
+                uint32_t kk = 0;
+#pragma unroll
+                for (uint32_t step = 16; step > 0; step >>= 1) {
+                    const uint32_t e = __shfl_sync(kFullMask, incl, kk + step - 1);
+                    if (e <= q) kk += step;
+                }
+                kk = min(kk, 31u);
+                const uint32_t sk = __shfl_sync(kFullMask, s, kk);
+                const uint32_t ek = __shfl_sync(kFullMask, excl, kk);
+                const double ak = __shfl_sync(kFullMask, a, kk);
+                const uint32_t j = sk + (q - ek);
+                uint32_t col = kEmptyCol;
+                double prod = 0.0;
+                if (valid) {
+                    col = __ldg(op.b_col + j);
+                    prod = __dmul_rn(ak, __ldg(op.b_val + j));
+                }
+                // products of a single A nonzero have distinct columns: no ordering inside the chunk
+                const uint32_t k0 = __shfl_sync(kFullMask, kk, 0);
+                const bool single = __all_sync(kFullMask, !valid || kk == k0);
+                int slot = -1;
+                uint32_t rank = 0;
+                if (dense) {
+                    const uint32_t d = col - c0;
+                    if (valid) {
+                        if (d < kTaskDense) slot = (int)d;
+                        else bad = true;
+                    }
+                    if (!single) rank = __popc(__match_any_sync(kFullMask, slot) & lanemask_lt());
+                } else {
+                    uint32_t leader = lane;
+                    if (!single) {
+                        const uint32_t m = __match_any_sync(kFullMask, col);
+                        rank = __popc(m & lanemask_lt());
+                        leader = __ffs(m) - 1;
+                    }
+                    if (valid && rank == 0) {
+                        uint32_t h = hash32(col) & tmask;
+                        for (uint32_t probe = 0; probe < tsize; ++probe) {
+                            const uint32_t cur = keys[h];
+                            if (cur == col) { slot = (int)h; break; }
+                            if (cur == kEmptyCol) {
+                                const uint32_t old = atomicCAS(&keys[h], kEmptyCol, col);
+                                if (old == kEmptyCol || old == col) { slot = (int)h; break; }
+                            }
+                            h = (h + 1) & tmask;
+                        }
+                        if (slot < 0) bad = true;
+                    }
+                    if (!single) slot = __shfl_sync(kFullMask, slot, leader);
+                }
+                const uint32_t maxr = single ? 0u : __reduce_max_sync(kFullMask, valid ? rank : 0u);
+                for (uint32_t r = 0; r <= maxr; ++r) {
+                    if (valid && rank == r && slot >= 0) accumulate(&vals[slot], prod);
+                    __syncwarp();
+                }
+            }
+        }
+
+        // emit in slot order (column order for a dense task), resetting the table
+        const bool any_bad = __any_sync(kFullMask, bad);
+        uint32_t cnt = 0;
+        for (uint32_t i = 0; i < tsize; i += 32) cnt += __popc(__ballot_sync(kFullMask, vbits[i + lane] != kNoValue));
+        uint64_t base = it.out_off;
+        if (base == kClaimBit) {
+            uint64_t b = ~0ull;
+            if (lane == 0) {
+                b = any_bad ? ~0ull : claim_output(op, out, row, cnt);
+                if (b == ~0ull) {  // rerun this task exactly
+                    const uint32_t f = atomicAdd(out.fail_count, 1u);
+                    out.fail_list[f] = t;
+                }
+            }
+            base = __shfl_sync(kFullMask, b, 0);
+        } else if (any_bad) {
+            if (lane == 0) atomicOr(overflow, 1u);  // exact sizes cannot overflow: report an internal error
+            base = ~0ull;
+        }
+        if (out.item_count && lane == 0) out.item_count[t] = base == ~0ull ? 0u : cnt;
+        uint64_t o = base;
+        for (uint32_t i = 0; i < tsize; i += 32) {
+            const uint32_t sidx = i + lane;
+            const bool occ = vbits[sidx] != kNoValue;
+            const uint32_t m = __ballot_sync(kFullMask, occ);
+            if (occ) {
+                if (base != ~0ull) write_entry(op, out, o + __popc(m & lanemask_lt()), row,
+                                               dense ? c0 + sidx : keys[sidx], vals[sidx]);
+                vbits[sidx] = kNoValue;
+                if (!dense) keys[sidx] = kEmptyCol;
+            }
+            o += __popc(m);
+        }
+        __syncwarp();
+    }
+}
+
+void launch_warp_tasks(const Operands& op, const PartItem* tasks, uint32_t ntasks, const OutputView& out,
+                       uint32_t* work_counter, uint32_t* overflow, int num_sms, cudaStream_t st) {
+    if (ntasks == 0) return;
+    const size_t smem = kTaskWarps * kTaskBytes;
+    PTC_CUDA(cudaMemsetAsync(work_counter, 0, sizeof(uint32_t), st));
+    int per_sm = 1;
+    PTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, warp_task_kernel, kTaskWarps * 32, smem));
+    per_sm = per_sm < 1 ? 1 : per_sm;
+    const uint32_t grid = (uint32_t)std::min<uint64_t>((ntasks + kTaskWarps - 1) / kTaskWarps, (uint64_t)num_sms * per_sm);
+    warp_task_kernel<<<grid, kTaskWarps * 32, smem, st>>>(op, tasks, ntasks, out, work_counter, overflow);
+    count_launch();
+    PTC_CHECK_LAUNCH();
+}
+
+// ---------------------------------------------------------------------------------------------
 // numeric pass for the other rows: one block per part (a row's columns in fine panels [p0, p1)).
 // A dense part indexes its accumulator by column directly; a sparse part uses an open-addressing
 // table.  Both live in the same shared-memory region.

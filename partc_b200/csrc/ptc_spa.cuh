@@ -25,6 +25,19 @@ void launch_small_rows(bool numeric, const Operands& op, const uint32_t* rows, u
 void launch_sym_bitmap(const Operands& op, const uint32_t* rows, uint32_t nrows, uint32_t* panel_cnt, uint64_t* row_d,
                        uint32_t* work_counter, int num_sms, cudaStream_t st);
 
+// largest exact output count of a sparse warp task, and its table bounds (log2 slots)
+uint32_t warp_task_capacity();
+uint32_t warp_task_min_bits();
+uint32_t warp_task_max_bits();
+// column width of a dense warp task
+uint32_t warp_task_dense_columns();
+// rows whose A nonzeros number at most this go to warp tasks (they rescan the row once per task)
+constexpr uint32_t kWarpTaskMaxLen = 4096;
+
+// other rows, numeric: one warp per task (a row's columns in fine panels [p0, p1))
+void launch_warp_tasks(const Operands& op, const PartItem* tasks, uint32_t ntasks, const OutputView& out,
+                       uint32_t* work_counter, uint32_t* overflow, int num_sms, cudaStream_t st);
+
 // other rows, numeric: one block per part
 void launch_hash_parts(const Operands& op, const PartItem* parts, uint32_t nparts, const OutputView& out,
                        uint32_t* work_counter, uint32_t* overflow, int num_sms, cudaStream_t st);
@@ -56,8 +69,10 @@ void launch_esc_fold(const Operands& op, const OutputView& out, const uint64_t* 
                      const uint64_t* row_off, const double* sorted, cudaStream_t st);
 // out[pos[i]] = i wherever flag[i] (pos = exclusive scan of flag)
 void launch_compact_indices(const uint32_t* flag, const uint32_t* pos, uint64_t n, uint32_t* out, cudaStream_t st);
-// key[i] = ~row_flops[rows[i]] (descending-work sort key)
-void launch_work_keys(const uint32_t* rows, uint64_t n, const uint64_t* row_flops, uint64_t* key, cudaStream_t st);
+// key[i] = (row has more than max_len A nonzeros) << 40 | ~row_flops[rows[i]] (low 40 bits): sorted,
+// the rows for warp tasks come first, each group largest first
+void launch_work_keys(const uint32_t* rows, uint64_t n, const uint64_t* row_flops, const uint32_t* row_start,
+                      uint32_t max_len, uint64_t* key, cudaStream_t st);
 // How a large row is cut into parts, from its exact output count per fine panel: windows of
 // dense_panels panels holding at least dense_min entries per panel become dense parts; the
 // other panels are grouped greedily into open-addressing parts of at most cap entries.
@@ -66,6 +81,8 @@ struct SplitRule {
     uint32_t dense_panels;  // 0 disables dense parts
     uint32_t dense_min;
     uint32_t min_bits;      // smallest open-addressing table, log2 slots
+    uint32_t max_bits;      // largest open-addressing table, log2 slots
+    uint32_t oversize_dense;  // 1: a single panel above cap becomes a dense part (else an error)
 };
 // number of parts of each big row; sets *oversize if one fine panel alone exceeds cap
 void launch_count_parts(const uint32_t* panel_cnt, uint64_t nbig, uint32_t npanels, SplitRule rule, uint32_t* nparts,
