@@ -192,6 +192,16 @@ def batch_member(seed: int) -> Workload:
     return Workload(f"batch{seed}", t, c, modes)
 
 
+def batch_members(n: int, procs: int = 0) -> list:
+    """Members 0..n-1 of the uneven batch, generated by ``procs`` worker processes (spawned, so a
+    process that already uses CUDA may call this)."""
+    if procs <= 1:
+        return [batch_member(s) for s in range(n)]
+    import multiprocessing as mp
+    with mp.get_context("spawn").Pool(procs) as pool:
+        return pool.map(batch_member, range(n), chunksize=16)
+
+
 def sizer_member(seed: int, nnz_scale: float = 1.0) -> Workload:
     """One training contraction for the learned sizer: 3-D or 4-D, dims 1k-20k (a 4-D tensor
     keeps one short mode of 8-63, as FROSTT 4-D tensors do), nnz log-uniform in [100k, 5M]
