@@ -180,9 +180,174 @@ def cpu_arm(w, target_flops, steps, warmup):
                    "sample_mult_adds": sflops, "seconds": t}
 
 
+def cpu_arm_batch(n_items, target_seconds, steps, warmup):
+    """The reference path on whole members of the uneven batch (seed order, every member whose
+    products the reference finishes quickly), until about target_seconds of work per step."""
+    import oracle
+    from partc_b200 import gen
+    kind = "reference" if os.path.exists(oracle.REF_BIN) else "port"
+    members = []
+    for seed in range(n_items):
+        w = gen.batch_member(seed)
+        if w.tensor.nnz > 1:
+            members.append(w)
+        if len(members) >= 64:
+            break
+    rates = []
+    used = 0
+    with tempfile.TemporaryDirectory() as td:
+        for rep in range(warmup + steps):
+            fl, sec = 0, 0.0
+            for i, w in enumerate(members):
+                st = oracle.contract(w.tensor, None, w.c, w.modes, mode=oracle.FLOPS_ONLY)
+                if st["flops"] == 0 or st["flops"] > 2e8:
+                    continue
+                sub = os.path.join(td, f"m{i}")
+                os.makedirs(sub, exist_ok=True)
+                keep = np.ones(w.tensor.nnz, dtype=bool)
+                r = run_reference_once(w, keep, sub) if kind == "reference" else run_port_once(w, keep)
+                fl += st["flops"]
+                sec += r["t_wall"]
+                used = i + 1
+                if sec > target_seconds:
+                    break
+            if rep >= warmup:
+                rates.append(fl / sec)
+    value = statistics.median(rates)
+    sample = (f"whole members of the uneven batch in seed order (the first {used} seeds, members above 2e8 "
+              f"mult-adds skipped), about {target_seconds:.0f} s of reference time per step; the reference's "
+              f"loops use one thread (fksCuckooTC.hpp:171-173)")
+    return value, {"value": value, "unit": "mult-adds/s", "cores": 1, "kind": kind, "sample": sample,
+                   "seconds": target_seconds}
+
+
 # ---------------------------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------------------------
+
+def run_batch(args, rank, world, local):
+    """One step = ptc_batch_contract over the uneven batch (members 0..n-1 of gen.batch_member),
+    inputs resident in HBM, outputs produced wave by wave and discarded; beside it the same members
+    contracted one ptc_contract call each (two-phase, outputs freed)."""
+    import torch
+    from partc_b200 import _lib, gen
+    from partc_b200 import dist as pdist
+    n = args.batch_items
+    work = gen.batch_members(n, procs=min(16, os.cpu_count() or 1))
+    dev = f"cuda:{local}"
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+    idx_cat = np.concatenate([w.tensor.idx.reshape(-1) for w in work]).view(np.int32)
+    val_cat = np.concatenate([w.tensor.vals for w in work])
+    di = torch.from_numpy(idx_cat).to(dev)
+    dv = torch.from_numpy(val_cat).to(dev)
+    keep = []
+
+    def make_items(ibase, vbase, loc):
+        items = (_lib.BatchItem * n)()
+        io = vo = 0
+        for i, w in enumerate(work):
+            t = w.tensor
+            d = np.ascontiguousarray(t.dims, dtype=np.uint32)
+            keep.append(d)
+            items[i].A = _lib.Coo(t.order, loc, t.nnz, ibase + 4 * io, vbase + 8 * vo, d.ctypes.data)
+            items[i].c = w.c
+            for j, m in enumerate(w.modes):
+                items[i].a_modes[j] = m
+            io += t.nnz * t.order
+            vo += t.nnz
+        return items
+
+    items = make_items(di.data_ptr(), dv.data_ptr(), _lib.PTC_DEVICE)
+    opts = dict(device=local, stream=stream.cuda_stream, path=args.path)
+    sizes = {}
+
+    def sink(i, t):
+        sizes[i] = (t.nnz, t.order)
+
+    _, st0 = _lib.batch_contract(items, outputs="sink", sink=sink, output_location="device", **opts)
+    M, R = st0["mult_adds"], st0["out_nnz"]
+    out_bytes = sum(k * (4 * o + 8) for k, o in sizes.values())
+    for _ in range(max(0, args.warmup - 1)):
+        _lib.batch_contract(items, outputs="none", **opts)
+    torch.cuda.synchronize()
+    pdist.barrier()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    stats = []
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            stats.append(_lib.batch_contract(items, outputs="none", **opts)[1])
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    pdist.barrier()
+    ms = pdist.max_over_ranks(ev0.elapsed_time(ev1), device=dev)
+    value = pdist.job_throughput(M, args.steps, world, ms * 1e-3)
+    na = int(sum(w.tensor.nnz for w in work))
+    alg = 12 * na + 12 * M + out_bytes
+    t_num = statistics.mean(s["t_numeric_ms"] for s in stats) * 1e-3
+    peak, peak_kind = measured_hbm_peak()
+    roofline = {"bound": "hbm", "achieved": alg / t_num / 1e9, "peak": peak, "unit": "GB/s",
+                "frac": alg / t_num / 1e9 / peak, "peak_source": peak_kind,
+                "kernel": "numeric pass of every wave (graph launches)", "algorithmic_bytes": alg,
+                "numeric_ms": t_num * 1e3, "traffic": None}
+
+    # the same members, one ptc_contract call each (two-phase path, device outputs freed)
+    loop = None
+    if args.per_contraction:
+        ev2 = torch.cuda.Event(enable_timing=True)
+        ev3 = torch.cuda.Event(enable_timing=True)
+        popts = dict(output_location="device", device=local, stream=stream.cuda_stream, path="two_phase")
+        ev2.record(stream)
+        fl = 0
+        for i in range(n):
+            try:
+                out, st = _lib.contract_coo(items[i].A, None, items[i].c, list(items[i].a_modes)[:items[i].A.order],
+                                            **popts)
+                _lib.free(out)
+                fl += st["mult_adds"]
+            except _lib.PtcError:
+                pass  # an item with no matching fiber or at most one nonzero: an error for a single call
+        ev3.record(stream)
+        torch.cuda.synchronize()
+        lms = ev2.elapsed_time(ev3)
+        loop = {"value": fl / (lms * 1e-3), "unit": "mult-adds/s", "ms": lms, "mult_adds": fl,
+                "calls": n, "path": "two_phase"}
+
+    # end to end: host inputs through the C ABI, per-item output counts read back
+    e2e = None
+    if args.e2e_steps > 0:
+        pi = torch.from_numpy(idx_cat).pin_memory()
+        pv = torch.from_numpy(val_cat).pin_memory()
+        hitems = make_items(pi.data_ptr(), pv.data_ptr(), _lib.PTC_HOST)
+        pdist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            _lib.batch_contract(hitems, outputs="none", device=local, stream=stream.cuda_stream, path=args.path)
+        el = pdist.max_over_ranks(time.perf_counter() - t0, device=dev)
+        e2e = {"value": pdist.job_throughput(M, args.e2e_steps, world, el), "unit": "mult-adds/s",
+               "h2d_bytes_per_step": int(idx_cat.nbytes + val_cat.nbytes), "d2h_bytes_per_step": 8 * n,
+               "note": "outputs stay in device waves (the library's sink interface); per-item counts come back",
+               "steps": args.e2e_steps, "ms_per_step": el / args.e2e_steps * 1e3}
+    if rank == 0:
+        line = {
+            "metric": "contraction mult-adds/s", "value": value, "unit": "mult-adds/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator partc_b200/gen.py batch_member, seeds 0..n-1)",
+            "config": {"workload": f"batch{n}", "items": n, "nnz": na, "path": args.path,
+                       "parallelism": f"replicas x{world}", "mult_adds_per_step": M, "out_nnz_per_step": R,
+                       "l2": "no flush needed: each step writes its outputs (>> 126 MB L2)"},
+            "phase_ms": {k: statistics.mean(s[k] for s in stats) for k in
+                         ("t_build_ms", "t_symbolic_ms", "t_numeric_ms", "t_d2h_ms", "t_total_ms")},
+            "batch_waves": stats[0]["batch_waves"], "rerun_items": stats[0]["rerun_items"],
+            "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
+            "roofline": roofline, "per_contraction": loop, "e2e": e2e, "cpu_baseline": None,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line))
+
 
 def main():
     ap = argparse.ArgumentParser()
@@ -195,15 +360,41 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-target-flops", type=float, default=6e7)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-items", type=int, default=4096)
+    ap.add_argument("--no-per-contraction", dest="per_contraction", action="store_false")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
     from partc_b200 import dist as pdist
     rank, world, local = pdist.rank_env()
 
+    if args.workload.startswith("batch") and args.impl == "ours":
+        if world > 1:
+            pdist.init("nccl", local)
+        run_batch(args, rank, world, local)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
     from partc_b200 import gen
-    w = gen.WORKLOADS[args.workload]()
-    t = w.tensor
+    w = None if args.workload.startswith("batch") else gen.WORKLOADS[args.workload]()
+    t = w.tensor if w is not None else None
+
+    if args.impl == "reference" and args.workload.startswith("batch"):
+        if not pdist.runs_reference_arm(rank):
+            return
+        steps = max(1, args.steps)
+        value, cb = cpu_arm_batch(args.batch_items, 10.0, steps, min(args.warmup, 1))
+        line = {"impl": "reference", "metric": "contraction mult-adds/s", "value": value, "unit": "mult-adds/s",
+                "n_gpus": args.gpus, "steps": steps, "warmup": min(args.warmup, 1), "ms_per_step": None,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded generator partc_b200/gen.py batch_member)",
+                "config": {"workload": f"batch{args.batch_items}", "parallelism": "host cores"},
+                "cpu_baseline": {k: cb[k] for k in ("kind", "cores", "sample", "value")},
+                "e2e": {"value": value, "unit": "mult-adds/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
 
     if args.impl == "reference":
         if not pdist.runs_reference_arm(rank):

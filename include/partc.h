@@ -100,7 +100,9 @@ typedef struct ptc_options {
     uint32_t hash_load_pct;         /* cuckoo table load factor in percent, 10-90 (default 75) */
     uint32_t batch_wave_mib;        /* ptc_batch_contract: device memory for one wave's outputs,
                                        MiB (default: 60% of the free memory) */
-    uint32_t reserved[3];
+    uint32_t warp_task_max_len;     /* large rows with at most this many A nonzeros use one warp per
+                                       column range, longer ones one block per part (default 4096) */
+    uint32_t reserved[2];
 } ptc_options;
 
 /* Per-call statistics; every time is measured with CUDA events on the call's stream. */
@@ -200,6 +202,27 @@ typedef void (*ptc_batch_sink)(void* user, uint32_t item, const ptc_tensor* out)
  */
 ptc_status ptc_batch_contract(const ptc_batch_item* items, uint32_t n, const ptc_options* opt,
                               ptc_tensor* outs, ptc_batch_sink sink, void* user, ptc_stats* stats);
+
+/* What ptc_autotune measured. */
+typedef struct ptc_tune_report {
+    uint32_t trials;     /* settings timed */
+    uint32_t repeats;    /* runs per setting (the median is kept) */
+    double default_ms;   /* median time of one run with the default knobs */
+    double best_ms;      /* median time of one run with the chosen knobs */
+    double reserved[4];
+} ptc_tune_report;
+
+/*
+ * Autotuner (no counterpart in the reference): picks the tuning knobs of ptc_options --
+ * panel_width (shared-table column ranges), small_max_products / warp_task_max_len /
+ * sort_max_avg_products (which accumulator, and so how many threads, each row gets) and
+ * hash_load_pct (cuckoo table load factor) -- for the given items by timing
+ * ptc_batch_contract on them (outputs discarded) under candidate settings, one knob at a time from
+ * the defaults, `repeats` runs per setting (median).  *best = *opt with the chosen knobs; results
+ * are identical under every setting, only the time changes.
+ */
+ptc_status ptc_autotune(const ptc_batch_item* items, uint32_t n, const ptc_options* opt, uint32_t repeats,
+                        ptc_options* best, ptc_tune_report* report);
 
 /* Number of CUDA devices the library can use (sm_100 class). */
 int ptc_device_count(void);

@@ -31,7 +31,7 @@ EXPORTS = [
     "ptc_tensor_free", "ptc_device_count", "ptc_train_options_init", "ptc_sizer_create", "ptc_sizer_load",
     "ptc_sizer_save", "ptc_sizer_free", "ptc_sizer_get_params", "ptc_sizer_set_params", "ptc_sizer_collect",
     "ptc_sizer_train", "ptc_sizer_predict", "ptc_sizer_gradients", "ptc_buffer_free",
-    "ptc_sizer_predict_noalloc", "ptc_batch_contract",
+    "ptc_sizer_predict_noalloc", "ptc_batch_contract", "ptc_autotune",
 ]
 SIZER_FEATURES = 16
 SIZER_PARAMS = 5313
@@ -60,7 +60,7 @@ class Options(C.Structure):
                 ("panel_width", C.c_uint32), ("hash_seed", C.c_uint64), ("sizer", C.c_void_p),
                 ("sort_rows", C.c_uint32), ("small_max_products", C.c_uint32),
                 ("sort_max_avg_products", C.c_uint32), ("hash_load_pct", C.c_uint32),
-                ("batch_wave_mib", C.c_uint32), ("reserved", C.c_uint32 * 3)]
+                ("batch_wave_mib", C.c_uint32), ("warp_task_max_len", C.c_uint32), ("reserved", C.c_uint32 * 2)]
 
 
 class Stats(C.Structure):
@@ -85,6 +85,13 @@ class BatchItem(C.Structure):
 
 
 SINK = C.CFUNCTYPE(None, C.c_void_p, C.c_uint32, C.POINTER(Tensor))
+
+
+class TuneReport(C.Structure):
+    _fields_ = [("trials", C.c_uint32), ("repeats", C.c_uint32), ("default_ms", C.c_double),
+                ("best_ms", C.c_double), ("reserved", C.c_double * 4)]
+
+TUNE_KNOBS = ("panel_width", "warp_task_max_len", "small_max_products", "sort_max_avg_products", "hash_load_pct")
 
 
 class TrainOptions(C.Structure):
@@ -124,6 +131,9 @@ def lib():
         L.ptc_batch_contract.argtypes = [C.POINTER(BatchItem), C.c_uint32, C.POINTER(Options), C.POINTER(Tensor),
                                          SINK, C.c_void_p, C.POINTER(Stats)]
         L.ptc_batch_contract.restype = C.c_int
+        L.ptc_autotune.argtypes = [C.POINTER(BatchItem), C.c_uint32, C.POINTER(Options), C.c_uint32,
+                                   C.POINTER(Options), C.POINTER(TuneReport)]
+        L.ptc_autotune.restype = C.c_int
         P, F = C.POINTER, C.c_float
         L.ptc_train_options_init.argtypes = [P(TrainOptions)]
         L.ptc_train_options_init.restype = None
@@ -272,6 +282,18 @@ def batch_items(work, keep: list, B_list=None):
             for j, m in enumerate(bm):
                 it.b_modes[j] = m
     return arr
+
+
+def autotune(items, repeats: int = 3, **opt):
+    """``ptc_autotune``: returns ``(knobs dict, report dict)``; pass the knobs to contract /
+    batch_contract as keyword options."""
+    o = options(**opt)
+    best = Options()
+    rep = TuneReport()
+    _check(lib().ptc_autotune(items, len(items), C.byref(o), repeats, C.byref(best), C.byref(rep)))
+    knobs = {k: int(getattr(best, k)) for k in TUNE_KNOBS}
+    return knobs, {"trials": rep.trials, "repeats": rep.repeats, "default_ms": rep.default_ms,
+                   "best_ms": rep.best_ms}
 
 
 def batch_contract(items, *, outputs: str = "arrays", sink=None, **opt):

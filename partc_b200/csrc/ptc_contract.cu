@@ -688,7 +688,7 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
     // large rows: warp tasks for rows of at most kWarpTaskMaxLen A nonzeros (panels of at most
     // a dense warp task's width), block parts for the others; each group largest first
     const uint32_t warp_len = (opt.panel_width == 0 || opt.panel_width <= warp_task_dense_columns())
-                                  ? kWarpTaskMaxLen : 0u;
+                                  ? (opt.warp_task_max_len ? opt.warp_task_max_len : kWarpTaskMaxLen) : 0u;
     if (n_big > 0) {
         uint64_t* wkey = ar.alloc<uint64_t>(n_big);
         launch_work_keys(pl.big_rows, n_big, pl.row_flops, op.row_start, warp_len, wkey, st);
@@ -1781,35 +1781,126 @@ ptc_status ptc_self_contract(const uint32_t* hedges, const double* vals, uint32_
     return ptc_contract(&A, nullptr, c, dim_tc, dim_tc, opt, out, stats);
 }
 
+}  // extern "C"
+
+namespace ptc {
+namespace {
+
+// The items of a batch call, checked.
+std::vector<BatchItemHost> batch_host_items(const ptc_batch_item* items, uint32_t n, uint32_t& location) {
+    PTC_REQUIRE(items != nullptr || n == 0, PTC_ERR_INVALID_ARGUMENT, "items is null");
+    std::vector<BatchItemHost> hi(n);
+    location = PTC_HOST;
+    for (uint32_t i = 0; i < n; ++i) {
+        const ptc_batch_item& it = items[i];
+        const bool self = it.B.idx == nullptr && it.B.nnz == 0 && it.B.dims == nullptr;
+        BatchItemHost& h = hi[i];
+        h.A = &it.A;
+        h.self = self;
+        h.B = self ? &it.A : &it.B;
+        h.c = it.c;
+        h.a_modes = it.a_modes;
+        h.b_modes = self ? it.a_modes : it.b_modes;
+        const std::string where = "item " + std::to_string(i) + ": ";
+        validate_pair(h.A, h.B, h.c, h.a_modes, h.b_modes, where);
+        h.fa = h.A->order - h.c;
+        h.fb = h.B->order - h.c;
+        if (i == 0) location = it.A.location;
+        PTC_REQUIRE(h.A->location == location && h.B->location == location, PTC_ERR_INVALID_ARGUMENT,
+                    where + "every input of a batch must be in the same memory");
+    }
+    return hi;
+}
+
+// Median time (ms, the calls' own event clocks) of `repeats` discarded-output runs.
+double time_batch(const std::vector<BatchItemHost>& hi, uint32_t location, const ptc_options& opt, uint32_t repeats) {
+    BatchTarget tg;
+    tg.ids.resize(hi.size());
+    for (uint32_t i = 0; i < hi.size(); ++i) tg.ids[i] = i;
+    std::vector<double> t;
+    for (uint32_t r = 0; r < repeats; ++r) {
+        ptc_stats st;
+        std::memset(&st, 0, sizeof(st));
+        batch_impl(hi, location, opt, false, tg, st);
+        t.push_back(st.t_total_ms);
+    }
+    std::sort(t.begin(), t.end());
+    return t[t.size() / 2];
+}
+
+}  // namespace
+}  // namespace ptc
+
+extern "C" {
+
+ptc_status ptc_autotune(const ptc_batch_item* items, uint32_t n, const ptc_options* opt_in, uint32_t repeats,
+                        ptc_options* best_out, ptc_tune_report* report) {
+    using namespace ptc;
+    try {
+        PTC_REQUIRE(best_out != nullptr && n > 0, PTC_ERR_INVALID_ARGUMENT, "need items and an output");
+        ptc_options opt = resolve_options(opt_in);
+        uint32_t location = PTC_HOST;
+        const std::vector<BatchItemHost> hi = batch_host_items(items, n, location);
+        repeats = std::max(1u, repeats);
+        time_batch(hi, location, opt, 1);  // warm-up: pool memory, code loading
+        ptc_tune_report rep;
+        std::memset(&rep, 0, sizeof(rep));
+        rep.repeats = repeats;
+        double best = time_batch(hi, location, opt, repeats);
+        rep.default_ms = best;
+        rep.trials = 1;
+        // one knob at a time, in the order of their expected effect; 0 = the default
+        struct Knob {
+            uint32_t ptc_options::*field;
+            std::vector<uint32_t> values;
+        };
+        const std::vector<Knob> knobs = {
+            {&ptc_options::panel_width, {0, 64, 128, 256, 512, 1024}},
+            {&ptc_options::warp_task_max_len, {0, 1024, 16384}},
+            {&ptc_options::small_max_products, {0, 128, 256}},
+            {&ptc_options::sort_max_avg_products, {0, 8, 16, 64}},
+            {&ptc_options::hash_load_pct, {0, 50, 90}},
+        };
+        const uint32_t user_panel = opt.panel_width;
+        for (const Knob& k : knobs) {
+            if (k.field == &ptc_options::panel_width && user_panel != 0) continue;  // the caller fixed it
+            const uint32_t start = opt.*k.field;
+            for (uint32_t v : k.values) {
+                if (v == start) continue;
+                ptc_options cand = opt;
+                cand.*k.field = v;
+                const double t = time_batch(hi, location, cand, repeats);
+                ++rep.trials;
+                if (t < best) {
+                    best = t;
+                    opt = cand;
+                }
+            }
+        }
+        rep.best_ms = best;
+        *best_out = opt;
+        if (report) *report = rep;
+        g_last_error.clear();
+        return PTC_OK;
+    } catch (const Error& e) {
+        set_last_error(e.status, e.msg);
+        return e.status;
+    } catch (...) {
+        set_last_error(PTC_ERR_INTERNAL, "unexpected exception");
+        return PTC_ERR_INTERNAL;
+    }
+}
+
 ptc_status ptc_batch_contract(const ptc_batch_item* items, uint32_t n, const ptc_options* opt_in, ptc_tensor* outs,
                               ptc_batch_sink sink, void* user, ptc_stats* stats_out) {
     using namespace ptc;
     try {
-        PTC_REQUIRE(items != nullptr || n == 0, PTC_ERR_INVALID_ARGUMENT, "items is null");
         const ptc_options opt = resolve_options(opt_in);
         ptc_stats stats;
         std::memset(&stats, 0, sizeof(stats));
         g_launches = 0;
-        std::vector<BatchItemHost> hi(n);
         uint32_t location = PTC_HOST;
-        for (uint32_t i = 0; i < n; ++i) {
-            const ptc_batch_item& it = items[i];
-            const bool self = it.B.idx == nullptr && it.B.nnz == 0 && it.B.dims == nullptr;
-            BatchItemHost& h = hi[i];
-            h.A = &it.A;
-            h.self = self;
-            h.B = self ? &it.A : &it.B;
-            h.c = it.c;
-            h.a_modes = it.a_modes;
-            h.b_modes = self ? it.a_modes : it.b_modes;
-            const std::string where = "item " + std::to_string(i) + ": ";
-            validate_pair(h.A, h.B, h.c, h.a_modes, h.b_modes, where);
-            h.fa = h.A->order - h.c;
-            h.fb = h.B->order - h.c;
-            if (i == 0) location = it.A.location;
-            PTC_REQUIRE(h.A->location == location && h.B->location == location, PTC_ERR_INVALID_ARGUMENT,
-                        where + "every input of a batch must be in the same memory");
-        }
+        const std::vector<BatchItemHost> hi = batch_host_items(items, n, location);
         BatchTarget tg;
         tg.outs = outs;
         tg.sink = sink;
