@@ -42,6 +42,8 @@ constexpr uint32_t kEscMaxAvgProducts = 32;
 constexpr uint32_t kDenseMinFraction = 5;
 // largest product count the sort-based accumulator buffers (32 bytes per product)
 constexpr uint64_t kEscMaxProducts = 256ull << 20;
+// largest per-fiber panel table (fibers x (panels + 1) offsets)
+constexpr uint64_t kPanelTableBytes = 4ull << 30;
 
 KeySpec make_keyspec(const uint32_t* dims, const uint32_t* modes, uint32_t n) {
     KeySpec k;
@@ -706,7 +708,8 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
 
     // fine column panels: B fibers are split at multiples of W so a row can be cut into parts
     // that each fit one shared-memory table (W <= table capacity, so a part always fits).  The
-    // per-fiber panel table is kept within 1 GiB (wider panels, else binary searches in the fiber).
+    // per-fiber panel table is built when it fits kPanelTableBytes (else binary searches in the
+    // fiber find a part's entries).
     PTC_REQUIRE(ncols <= sym_bitmap_max_cols(), PTC_ERR_INVALID_ARGUMENT,
                 "more than 1.5M distinct B free keys in one contraction is not supported yet");
     auto table_bytes = [&](uint32_t w) { return nfib * ((ncols + w - 1) / w + 1) * 4; };
@@ -723,7 +726,7 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
     const uint32_t P = pl.P;
     stats.panel_width = W;
     uint32_t* panel_off = nullptr;
-    if (P > 1 && table_bytes(W) <= (1ull << 30)) {
+    if (P > 1 && table_bytes(W) <= kPanelTableBytes) {
         panel_off = ar.alloc<uint32_t>(nfib * (uint64_t)(P + 1));
         launch_panel_offsets(op.b_col, F.b_fib, op.fib_start, nb, P, pl.log2w, panel_off, st);
     }
@@ -746,6 +749,10 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
     br.min_bits = hash_part_min_bits();
     br.max_bits = 13;
     br.oversize_dense = 0;
+    if (pl.learned) {  // predicted sizes: every open-addressing table at its largest, for slack
+        wr.min_bits = wr.max_bits;
+        br.min_bits = br.max_bits;
+    }
 
     // symbolic: exact output nnz of the small rows (both paths) and of the large rows (per fine
     // panel; two-phase path only -- the learned path predicts those)
@@ -1374,9 +1381,15 @@ void batch_impl(const std::vector<BatchItemHost>& items, uint32_t location, cons
     const bool keep_device = tg.outs && opt.output_location == PTC_DEVICE;
     uint64_t budget = (uint64_t)opt.batch_wave_mib << 20;
     if (budget == 0) {
+        // free device memory, counting what the stream-ordered pool holds without using it
         size_t free_b = 0, total_b = 0;
         PTC_CUDA(cudaMemGetInfo(&free_b, &total_b));
-        budget = (uint64_t)(free_b * 0.6);
+        cudaMemPool_t pool;
+        uint64_t reserved = 0, used = 0;
+        PTC_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev.device));
+        PTC_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
+        PTC_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used));
+        budget = (uint64_t)((free_b + (reserved > used ? reserved - used : 0)) * 0.6);
     }
     if (keep_device) budget = UINT64_MAX;  // every output stays: one wave
     std::vector<uint32_t> wave_item{0};
