@@ -91,7 +91,9 @@ typedef struct ptc_options {
     uint64_t hash_seed;        /* seed of the cuckoo hash family */
     const ptc_sizer* sizer;    /* PTC_PATH_LEARNED: trained sizer (NULL = built-in weights) */
     uint32_t sort_rows;        /* 1: rows of the output in increasing free-key order and every
-                                  row in increasing column order (canonical COO) */
+                                  row in increasing column order (canonical COO); runs the
+                                  two-phase path and one sort of the entries (about 24 extra bytes
+                                  of device memory per output entry); single contractions only */
     /* tuning knobs (0 = default) */
     uint32_t small_max_products;    /* rows with at most this many products use the one-warp
                                        accumulator (<= 512; default 512) */

@@ -181,6 +181,44 @@ void launch_panel_offsets(const uint32_t* b_col, const uint32_t* b_fib, const ui
 
 namespace ptc {
 
+// canonical output order: key[e] = row_of[e] << colbits | col_of[e], perm[e] = e
+__global__ void entry_keys_kernel(const uint32_t* __restrict__ row_of, const uint32_t* __restrict__ col_of, uint64_t n,
+                                  uint32_t colbits, uint64_t* __restrict__ key, uint32_t* __restrict__ perm) {
+    const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    key[e] = ((uint64_t)row_of[e] << colbits) | col_of[e];
+    perm[e] = (uint32_t)e;
+}
+
+void launch_entry_keys(const uint32_t* row_of, const uint32_t* col_of, uint64_t n, uint32_t colbits, uint64_t* key,
+                       uint32_t* perm, cudaStream_t st) {
+    if (n == 0) return;
+    entry_keys_kernel<<<ceil_div_u32(n, 256), 256, 0, st>>>(row_of, col_of, n, colbits, key, perm);
+    count_launch();
+    PTC_CHECK_LAUNCH();
+}
+
+// dst tuple e = src tuple perm[e] (od u32 each)
+__global__ void gather_tuples_kernel(const uint32_t* __restrict__ src, const uint32_t* __restrict__ perm, uint64_t n,
+                                     uint32_t od, uint32_t* __restrict__ dst) {
+    const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const uint64_t s = perm[e];
+    for (uint32_t m = 0; m < od; ++m) dst[e * od + m] = src[s * od + m];
+}
+
+void launch_gather_tuples(const uint32_t* src, const uint32_t* perm, uint64_t n, uint32_t od, uint32_t* dst,
+                          cudaStream_t st) {
+    if (n == 0) return;
+    gather_tuples_kernel<<<ceil_div_u32(n, 256), 256, 0, st>>>(src, perm, n, od, dst);
+    count_launch();
+    PTC_CHECK_LAUNCH();
+}
+
+}  // namespace ptc
+
+namespace ptc {
+
 // ---------------------------------------------------------------------------------------------
 // batches: every item keeps its own mode lists and key range (ItemSpec, ptc_build.cuh)
 // ---------------------------------------------------------------------------------------------

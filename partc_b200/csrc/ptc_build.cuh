@@ -19,6 +19,12 @@ void launch_row_flops(const uint64_t* poff, const uint32_t* row_start, uint64_t 
 void launch_panel_offsets(const uint32_t* b_col, const uint32_t* b_fib, const uint32_t* fib_start, uint64_t nb,
                           uint32_t P, uint32_t log2w, uint32_t* off, cudaStream_t st);
 
+// ---- canonical output order ----
+void launch_entry_keys(const uint32_t* row_of, const uint32_t* col_of, uint64_t n, uint32_t colbits, uint64_t* key,
+                       uint32_t* perm, cudaStream_t st);
+void launch_gather_tuples(const uint32_t* src, const uint32_t* perm, uint64_t n, uint32_t od, uint32_t* dst,
+                          cudaStream_t st);
+
 // ---- batches ----
 
 // One side (A = 0, B = 1) of a batch item, as the device reads it: the item's COO arrays, its modes

@@ -952,7 +952,8 @@ void contract_impl(const ptc_coo* A, const ptc_coo* Bin, uint32_t c, const uint3
     const Knobs kn = knobs_of(opt);
     Front F = front_single(A, B, self, c, a_modes, b_modes, opt, kn, ar, ev, stats);
 
-    const bool learned = opt.path == PTC_PATH_LEARNED && collect == nullptr;
+    // the canonical order (sort_rows) runs on exact offsets: the two-phase path
+    const bool learned = opt.path == PTC_PATH_LEARNED && collect == nullptr && !opt.sort_rows;
     const SizerHost* sizer = nullptr;
     if (learned) {
         sizer = opt.sizer ? sizer_host(opt.sizer) : default_sizer();
@@ -978,6 +979,10 @@ void contract_impl(const ptc_coo* A, const ptc_coo* Bin, uint32_t c, const uint3
     PTC_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&ov.idx), std::max<uint64_t>(capacity * od, 1) * sizeof(uint32_t), st));
     PTC_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&ov.val), std::max<uint64_t>(capacity, 1) * sizeof(double), st));
     uint64_t out_nnz = pl.exact_nnz;
+    if (opt.sort_rows) {  // canonical order: remember every entry's row and column
+        ov.row_of = ar.alloc<uint32_t>(std::max<uint64_t>(capacity, 1));
+        ov.col_of = ar.alloc<uint32_t>(std::max<uint64_t>(capacity, 1));
+    }
     try {
         if (learned) {
             // the small and sort-based rows fill [0, exact_nnz); the large rows claim after them
@@ -1006,6 +1011,26 @@ void contract_impl(const ptc_coo* A, const ptc_coo* Bin, uint32_t c, const uint3
         if (learned) {
             out_nnz = learned_reruns(op, groups, pl.big_rows, pl.n_big, pl.pred, pl.rule[1], ov, pl.work_counter,
                                      op.err, dev.num_sms, op.nrows, ar, stats);
+        }
+        if (opt.sort_rows && out_nnz > 1) {
+            // rows in increasing free-key order, every row in increasing column order: one sort
+            // of the entries by (row, column), then the tuples and values follow the permutation
+            const uint32_t colbits = (uint32_t)bits_for_space(std::max<uint64_t>(op.ncols, 1));
+            const int keybits = (int)colbits + bits_for_space(std::max<uint64_t>(op.nrows, 1));
+            uint64_t* key = ar.alloc<uint64_t>(out_nnz);
+            uint32_t* perm = ar.alloc<uint32_t>(out_nnz);
+            launch_entry_keys(ov.row_of, ov.col_of, out_nnz, colbits, key, perm, st);
+            radix_sort_pairs(key, perm, out_nnz, 0, keybits, ar);
+            uint32_t* idx2 = nullptr;
+            double* val2 = nullptr;
+            PTC_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&idx2), out_nnz * od * sizeof(uint32_t), st));
+            PTC_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&val2), out_nnz * sizeof(double), st));
+            launch_gather_tuples(ov.idx, perm, out_nnz, od, idx2, st);
+            launch_gather<double>(ov.val, perm, out_nnz, val2, st);
+            PTC_CUDA(cudaFreeAsync(ov.idx, st));
+            PTC_CUDA(cudaFreeAsync(ov.val, st));
+            ov.idx = idx2;
+            ov.val = val2;
         }
         PTC_CUDA(cudaEventRecord(ev.ev[EV_NUM], st));
         PTC_REQUIRE(read_scalar(op.err, st) == 0, PTC_ERR_INTERNAL,
@@ -1909,6 +1934,7 @@ ptc_status ptc_batch_contract(const ptc_batch_item* items, uint32_t n, const ptc
     using namespace ptc;
     try {
         const ptc_options opt = resolve_options(opt_in);
+        PTC_REQUIRE(!opt.sort_rows, PTC_ERR_INVALID_ARGUMENT, "sort_rows is for single contractions");
         ptc_stats stats;
         std::memset(&stats, 0, sizeof(stats));
         g_launches = 0;

@@ -94,6 +94,8 @@ struct OutputView {
     uint32_t* fail_list = nullptr;      // work items to rerun exactly
     uint32_t* fail_count = nullptr;
     uint32_t* item_count = nullptr;     // optional: entries written by each work item
+    uint32_t* row_of = nullptr;         // optional (canonical order): row of every entry
+    uint32_t* col_of = nullptr;         // optional (canonical order): column of every entry
 };
 
 // Take `n` entries at the cursor of the row's item; ~0 if they pass the item's end.  An
@@ -125,6 +127,10 @@ __device__ __forceinline__ void write_entry(const Operands& op, const OutputView
     }
     const uint32_t od = fa + fb;
     uint32_t* dst = out.idx + o * od;
+    if (out.row_of) {
+        out.row_of[o] = row;
+        out.col_of[o] = col;
+    }
     if (fa == 2 && fb == 2) {
         const uint2 r = *reinterpret_cast<const uint2*>(op.row_tuple + (uint64_t)row * 2);
         const uint2 c = *reinterpret_cast<const uint2*>(op.col_tuple + (uint64_t)col * 2);

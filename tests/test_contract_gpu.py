@@ -157,3 +157,15 @@ def test_dropin_driver(engine, oracle_mod, tmp_path):
     dims = (t.idx.max(axis=0) + 1).astype(np.uint32)
     o = oracle_mod.contract(gen.CooTensor(idx=t.idx, vals=t.vals, dims=dims), None, 2, [1, 2, 0, 3])
     assert nnz == o["nnz"]
+
+
+@pytest.mark.parametrize("path", ["two_phase", "learned"])
+def test_sort_rows_gives_canonical_order(engine, oracle_mod, path):
+    """sort_rows=1: rows in increasing free-key order, each row in increasing column order --
+    the lexicographic order of the output tuples when free keys follow the modes' order."""
+    t = gen.random_coo([80, 60, 300], 40000, [1.2, 1.0, 1.1], 21, "uniform01")
+    o = oracle_mod.contract(t, None, 1, [0, 1, 2])
+    idx, vals, _ = engine.contract(t, None, 1, [0, 1, 2], sort_rows=1, path=path)
+    assert_same_output(idx, vals, o["idx"], o["vals"], bit_exact=True)
+    order = np.lexsort(idx.T[::-1])
+    assert np.array_equal(order, np.arange(len(order)))
