@@ -742,6 +742,8 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
     wr.min_bits = warp_task_min_bits();
     wr.max_bits = warp_task_max_bits();
     wr.oversize_dense = 1;
+    wr.load_num = 1;
+    wr.load_den = 2;
     SplitRule& br = pl.rule[1];  // block parts
     br.cap = hash_part_capacity();
     br.dense_panels = dense_part_columns() >> pl.log2w;
@@ -749,6 +751,8 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
     br.min_bits = hash_part_min_bits();
     br.max_bits = 13;
     br.oversize_dense = 0;
+    br.load_num = 3;
+    br.load_den = 4;
     if (pl.learned) {  // predicted sizes: every open-addressing table at its largest, for slack
         wr.min_bits = wr.max_bits;
         br.min_bits = br.max_bits;

@@ -117,9 +117,9 @@ __device__ __forceinline__ uint32_t split_panels(const uint32_t* cnt, uint32_t P
             ++parts;
             before += acc;
         } else if (acc > 0) {
-            // table of at least acc / 0.75 slots, a power of two
+            // table of at least acc * load_den / load_num slots, a power of two
             uint32_t bits = rule.min_bits;
-            while (bits < rule.max_bits && ((uint64_t)3 << bits) < acc * 4) ++bits;
+            while (bits < rule.max_bits && ((uint64_t)rule.load_num << bits) < acc * rule.load_den) ++bits;
             emit(p0, p, before, bits << 1);
             ++parts;
             before += acc;

@@ -316,7 +316,8 @@ constexpr size_t kTaskBytes = kTaskDense * sizeof(double);  // shared memory per
 // the sparse layout keeps values in vals[0, 512) and keys in the bytes of vals[512, 768)
 static_assert(kTaskSlots * (sizeof(double) + sizeof(uint32_t)) <= kTaskBytes, "sparse layout fits a warp's region");
 
-uint32_t warp_task_capacity() { return kTaskSlots * 3 / 4; }  // load factor <= 0.75
+// load factor <= 0.5: linear probes stay short, and a warp waits for its longest one
+uint32_t warp_task_capacity() { return kTaskSlots / 2; }
 uint32_t warp_task_dense_columns() { return kTaskDense; }
 uint32_t warp_task_min_bits() { return 6; }                   // 64 slots: two per lane
 uint32_t warp_task_max_bits() { return 9; }
@@ -435,11 +436,13 @@ __global__ void __launch_bounds__(kTaskWarps * 32, 6)
             }
         }
 
-        // emit in slot order (column order for a dense task), resetting the table
+        // emit in slot order (column order for a dense task), resetting the table; the entry count
+        // is needed first only to claim an output range
         const bool any_bad = __any_sync(kFullMask, bad);
-        uint32_t cnt = 0;
-        for (uint32_t i = 0; i < tsize; i += 32) cnt += __popc(__ballot_sync(kFullMask, vbits[i + lane] != kNoValue));
         uint64_t base = it.out_off;
+        uint32_t cnt = 0;
+        if (base == kClaimBit || out.item_count)
+            for (uint32_t i = 0; i < tsize; i += 32) cnt += __popc(__ballot_sync(kFullMask, vbits[i + lane] != kNoValue));
         if (base == kClaimBit) {
             uint64_t b = ~0ull;
             if (lane == 0) {

@@ -83,6 +83,7 @@ struct SplitRule {
     uint32_t min_bits;      // smallest open-addressing table, log2 slots
     uint32_t max_bits;      // largest open-addressing table, log2 slots
     uint32_t oversize_dense;  // 1: a single panel above cap becomes a dense part (else an error)
+    uint32_t load_num, load_den;  // open-addressing tables at most load_num / load_den full
 };
 // number of parts of each big row; sets *oversize if one fine panel alone exceeds cap
 void launch_count_parts(const uint32_t* panel_cnt, uint64_t nbig, uint32_t npanels, SplitRule rule, uint32_t* nparts,
