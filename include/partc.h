@@ -205,6 +205,19 @@ typedef void (*ptc_batch_sink)(void* user, uint32_t item, const ptc_tensor* out)
 ptc_status ptc_batch_contract(const ptc_batch_item* items, uint32_t n, const ptc_options* opt,
                               ptc_tensor* outs, ptc_batch_sink sink, void* user, ptc_stats* stats);
 
+/*
+ * Read a FROSTT .tns file (one nonzero per line: d 1-based labels, then the value; '#' / '%'
+ * comment lines) on the GPU, as readTensor does with pigo (mtxTnsIO.cpp:30-65): same labels
+ * (minus one), same values (pigo's decimal arithmetic, bit for bit), each mode's size its largest
+ * label.  *out gets the tensor (order d, in opt->output_location memory; release with
+ * ptc_tensor_free) and dims[0..d) the mode sizes (dims must hold 16 entries).
+ */
+ptc_status ptc_read_tns(const char* path, const ptc_options* opt, ptc_tensor* out, uint32_t* dims);
+
+/* Write a tensor (host or device arrays) as .tns text: 1-based labels, values with 17
+ * significant digits (which read back to the same double). */
+ptc_status ptc_write_tns(const char* path, const ptc_tensor* t);
+
 /* What ptc_autotune measured. */
 typedef struct ptc_tune_report {
     uint32_t trials;     /* settings timed */

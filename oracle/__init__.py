@@ -107,6 +107,35 @@ def contract(A, B, c: int, a_modes, b_modes=None, mode: int = VALUES) -> dict:
     return out
 
 
+REF_IO_SO = os.path.join(HERE, "_ref", "libref_io.so")
+_refio = None
+
+
+def ref_read_tns(path: str) -> dict:
+    """The reference's own .tns reader (readTensor with pigo), compiled from its sources:
+    0-based labels [N, d], values, and mode sizes."""
+    global _refio
+    if _refio is None:
+        _refio = C.CDLL(REF_IO_SO)
+        _refio.ref_read_tns.argtypes = [C.c_char_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                        C.POINTER(C.POINTER(C.c_uint32)), C.POINTER(C.POINTER(C.c_uint32)),
+                                        C.POINTER(C.POINTER(C.c_double))]
+        _refio.ref_io_free.argtypes = [C.c_void_p]
+    d, n = C.c_uint32(), C.c_uint32()
+    ip, dp = C.POINTER(C.c_uint32)(), C.POINTER(C.c_uint32)()
+    vp = C.POINTER(C.c_double)()
+    _refio.ref_read_tns(path.encode(), C.byref(d), C.byref(n), C.byref(ip), C.byref(dp), C.byref(vp))
+    out = {"idx": _arr(ip, n.value * d.value, np.uint32).reshape(-1, d.value),
+           "vals": _arr(vp, n.value, np.float64), "dims": _arr(dp, d.value, np.uint32)}
+    for p in (ip, dp, vp):
+        _refio.ref_io_free(C.cast(p, C.c_void_p))
+    return out
+
+
+def ref_io_available() -> bool:
+    return os.path.exists(REF_IO_SO)
+
+
 def ref_available() -> bool:
     return os.path.exists(REF_SO)
 

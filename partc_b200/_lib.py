@@ -31,7 +31,7 @@ EXPORTS = [
     "ptc_tensor_free", "ptc_device_count", "ptc_train_options_init", "ptc_sizer_create", "ptc_sizer_load",
     "ptc_sizer_save", "ptc_sizer_free", "ptc_sizer_get_params", "ptc_sizer_set_params", "ptc_sizer_collect",
     "ptc_sizer_train", "ptc_sizer_predict", "ptc_sizer_gradients", "ptc_buffer_free",
-    "ptc_sizer_predict_noalloc", "ptc_batch_contract", "ptc_autotune",
+    "ptc_sizer_predict_noalloc", "ptc_batch_contract", "ptc_autotune", "ptc_read_tns", "ptc_write_tns",
 ]
 SIZER_FEATURES = 16
 SIZER_PARAMS = 5313
@@ -134,6 +134,10 @@ def lib():
         L.ptc_autotune.argtypes = [C.POINTER(BatchItem), C.c_uint32, C.POINTER(Options), C.c_uint32,
                                    C.POINTER(Options), C.POINTER(TuneReport)]
         L.ptc_autotune.restype = C.c_int
+        L.ptc_read_tns.argtypes = [C.c_char_p, C.POINTER(Options), C.POINTER(Tensor), C.c_void_p]
+        L.ptc_read_tns.restype = C.c_int
+        L.ptc_write_tns.argtypes = [C.c_char_p, C.POINTER(Tensor)]
+        L.ptc_write_tns.restype = C.c_int
         P, F = C.POINTER, C.c_float
         L.ptc_train_options_init.argtypes = [P(TrainOptions)]
         L.ptc_train_options_init.restype = None
@@ -282,6 +286,27 @@ def batch_items(work, keep: list, B_list=None):
             for j, m in enumerate(bm):
                 it.b_modes[j] = m
     return arr
+
+
+def read_tns(path: str, **opt):
+    """``ptc_read_tns`` (GPU parser): returns a ``gen.CooTensor`` with host numpy arrays."""
+    from partc_b200.gen import CooTensor
+    o = options(**opt)
+    out = Tensor()
+    dims = np.zeros(16, dtype=np.uint32)
+    _check(lib().ptc_read_tns(path.encode(), C.byref(o), C.byref(out), dims.ctypes.data))
+    d = out.order
+    idx, vals = _host_arrays(out)
+    return CooTensor(idx=idx.reshape(-1, d), vals=vals, dims=dims[:d].copy())
+
+
+def write_tns(path: str, t) -> None:
+    """``ptc_write_tns`` of a host tensor (``idx`` [nnz, d] uint32, ``vals``)."""
+    idx = np.ascontiguousarray(t.idx, dtype=np.uint32)
+    vals = np.ascontiguousarray(t.vals, dtype=np.float64)
+    tt = Tensor(idx.shape[1], PTC_HOST, idx.shape[0], idx.ctypes.data_as(C.POINTER(C.c_uint32)),
+                vals.ctypes.data_as(C.POINTER(C.c_double)), None)
+    _check(lib().ptc_write_tns(path.encode(), C.byref(tt)))
 
 
 def autotune(items, repeats: int = 3, **opt):
