@@ -225,6 +225,49 @@ def cpu_arm_batch(n_items, target_seconds, steps, warmup):
 # our arm
 # ---------------------------------------------------------------------------------------------
 
+def matricized_cusparse(w, dev, M):
+    """The reference's other baseline, matricize then SpGEMM (matricizedspGEMM.hpp:172-603), on
+    the GPU: A as a CSR matrix (rows = A's free keys, columns = contracted keys) times its
+    transpose-shaped B, through torch's CSR x CSR product (cuSPARSE SpGEMM), float64.  Timed with
+    CUDA events around the product only; a comparison point, not this library's path."""
+    import torch
+    t = w.tensor
+    dims = t.dims.astype(np.int64)
+    con, free = w.modes[:w.c], w.modes[w.c:]
+    ck = np.zeros(t.nnz, np.int64)
+    fk = np.zeros(t.nnz, np.int64)
+    for m in con:
+        ck = ck * dims[m] + t.idx[:, m]
+    for m in free:
+        fk = fk * dims[m] + t.idx[:, m]
+    _, ci = np.unique(ck, return_inverse=True)
+    _, fi = np.unique(fk, return_inverse=True)
+    nr, nc = int(fi.max()) + 1, int(ci.max()) + 1
+    try:
+        a = torch.sparse_coo_tensor(torch.from_numpy(np.stack([fi, ci])), torch.from_numpy(t.vals), (nr, nc),
+                                    device=dev).coalesce().to_sparse_csr()
+        b = torch.sparse_coo_tensor(torch.from_numpy(np.stack([ci, fi])), torch.from_numpy(t.vals), (nc, nr),
+                                    device=dev).coalesce().to_sparse_csr()
+        c = torch.sparse.mm(a, b)  # warm-up
+        nnz = int(c._nnz())
+        del c
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        c = torch.sparse.mm(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        del a, b, c
+        torch.cuda.empty_cache()
+        return {"value": M / (ms * 1e-3), "unit": "mult-adds/s", "ms": ms, "out_nnz": nnz,
+                "what": "torch CSR x CSR (cuSPARSE SpGEMM), f64, product only"}
+    except Exception as ex:  # e.g. the product's workspace does not fit the device
+        torch.cuda.empty_cache()
+        return {"value": None, "error": str(ex)[:200]}
+
+
 def run_batch(args, rank, world, local):
     """One step = ptc_batch_contract over the uneven batch (members 0..n-1 of gen.batch_member),
     inputs resident in HBM, outputs produced wave by wave and discarded; beside it the same members
@@ -355,12 +398,14 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--path", default="two_phase", choices=["two_phase", "learned"])
+    ap.add_argument("--path", default="learned", choices=["two_phase", "learned"])
+    ap.add_argument("--no-compare-paths", dest="compare_paths", action="store_false")
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-target-flops", type=float, default=6e7)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-items", type=int, default=4096)
+    ap.add_argument("--no-cusparse", dest="cusparse", action="store_false")
     ap.add_argument("--no-per-contraction", dest="per_contraction", action="store_false")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
@@ -454,6 +499,34 @@ def main():
     value = pdist.job_throughput(M, args.steps, world, ms * 1e-3)
     ms_step = ms / args.steps
 
+    # the other path, timed the same way (learned-sized against exact two-phase sizing)
+    other = "two_phase" if args.path == "learned" else "learned"
+    paths = {args.path: {"value": value, "ms_per_step": ms_step,
+                         "t_symbolic_ms": statistics.mean(s["t_symbolic_ms"] for s in stats),
+                         "rerun_rows": int(stats[0]["rerun_rows"]),
+                         "sizer_mean_abs_log2_err": stats[0]["sizer_mean_abs_log2_err"]}}
+    if args.compare_paths:
+        oopts = dict(opts, path=other)
+        for _ in range(2):
+            out, _ = _lib.contract_coo(coo, None, w.c, w.modes, **oopts)
+            _lib.free(out)
+        torch.cuda.synchronize()
+        pdist.barrier()
+        ost = []
+        ev0.record(stream)
+        for _ in range(args.steps):
+            out, st = _lib.contract_coo(coo, None, w.c, w.modes, **oopts)
+            _lib.free(out)
+            ost.append(st)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        oms = pdist.max_over_ranks(ev0.elapsed_time(ev1), device=f"cuda:{local}")
+        paths[other] = {"value": pdist.job_throughput(M, args.steps, world, oms * 1e-3),
+                        "ms_per_step": oms / args.steps,
+                        "t_symbolic_ms": statistics.mean(s["t_symbolic_ms"] for s in ost),
+                        "rerun_rows": int(ost[0]["rerun_rows"]),
+                        "sizer_mean_abs_log2_err": ost[0]["sizer_mean_abs_log2_err"]}
+
     # numeric pass roofline
     od = 2 * (t.order - w.c)
     alg_bytes = 12 * t.nnz + 12 * M + (4 * od + 8) * R
@@ -462,7 +535,8 @@ def main():
     peak, peak_kind = measured_hbm_peak()
     traffic = traffic_from_profile()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "peak_source": peak_kind, "kernel": "numeric pass (hash_part_kernel + small_rows_kernel<numeric>)",
+                "peak_source": peak_kind,
+                "kernel": "numeric pass (warp_task_kernel + hash_part_kernel + small_rows_kernel<numeric>)",
                 "algorithmic_bytes": alg_bytes, "numeric_ms": t_num * 1e3,
                 "traffic": traffic.get("bytes_per_launch") if traffic else None}
 
@@ -486,6 +560,8 @@ def main():
                "h2d_bytes_per_step": t.nnz * (4 * t.order + 8), "d2h_bytes_per_step": R * (4 * od + 8),
                "steps": args.e2e_steps, "ms_per_step": el / args.e2e_steps * 1e3}
 
+    cusparse = matricized_cusparse(w, f"cuda:{local}", M) if (args.cusparse and rank == 0 and world == 1) else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -508,6 +584,7 @@ def main():
                          ("t_build_ms", "t_symbolic_ms", "t_numeric_ms", "t_total_ms")},
             "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
             "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clk.summary(),
+            "matricized_cusparse": cusparse, "paths": paths,
         }
         print(json.dumps(line))
     if world > 1:
