@@ -310,9 +310,10 @@ void launch_sym_bitmap(const Operands& op, const uint32_t* rows, uint32_t nrows,
 // ---------------------------------------------------------------------------------------------
 
 constexpr int kTaskWarps = 4;                               // warps per block
-constexpr uint32_t kTaskDense = 1024;                       // columns of a dense task
+constexpr int kTaskBlocksPerSm = 8;                         // 32 resident warps per SM
+constexpr uint32_t kTaskDense = 768;                        // columns of a dense task
 constexpr uint32_t kTaskSlots = 512;                        // largest sparse table
-constexpr size_t kTaskBytes = kTaskDense * sizeof(double);  // shared memory per warp
+constexpr size_t kTaskBytes = kTaskDense * sizeof(double);  // shared memory per warp (6 KiB)
 // the sparse layout keeps values in vals[0, 512) and keys in the bytes of vals[512, 768)
 static_assert(kTaskSlots * (sizeof(double) + sizeof(uint32_t)) <= kTaskBytes, "sparse layout fits a warp's region");
 
@@ -322,7 +323,106 @@ uint32_t warp_task_dense_columns() { return kTaskDense; }
 uint32_t warp_task_min_bits() { return 6; }                   // 64 slots: two per lane
 uint32_t warp_task_max_bits() { return 9; }
 
-__global__ void __launch_bounds__(kTaskWarps * 32, 6)
+// One chunk of 32 products of a task: lane l takes product q0 + l of the packed stream.
+struct Chunk {
+    uint32_t kk;    // source lane (the A nonzero of this window)
+    uint32_t col;   // kEmptyCol past the end
+    double bval;
+};
+
+__device__ __forceinline__ Chunk load_chunk(const Operands& op, uint32_t q0, uint32_t total, uint32_t incl,
+                                            uint32_t s, uint32_t excl) {
+    Chunk c;
+    const uint32_t q = q0 + lane_id();
+    // source lane: number of lanes whose inclusive end is <= q
+    uint32_t kk = 0;
+#pragma unroll
+    for (uint32_t step = 16; step > 0; step >>= 1) {
+        const uint32_t e = __shfl_sync(kFullMask, incl, kk + step - 1);
+        if (e <= q) kk += step;
+    }
+    kk = min(kk, 31u);
+    const uint32_t sk = __shfl_sync(kFullMask, s, kk);
+    const uint32_t ek = __shfl_sync(kFullMask, excl, kk);
+    c.kk = kk;
+    c.col = kEmptyCol;
+    c.bval = 0.0;
+    if (q < total) {
+        const uint32_t j = sk + (q - ek);
+        c.col = __ldg(op.b_col + j);
+        c.bval = __ldg(op.b_val + j);
+    }
+    return c;
+}
+
+// Emit the warp's table: entries in slot order (column order for a dense task) from output
+// position `base`, resetting the table.  Four 32-slot groups at a time, so their tuple loads are
+// in flight together.  fa/fb > 0: the single-contraction layout with those free-mode counts.
+template <int FA, int FB>
+__device__ __forceinline__ void emit_table(const Operands& op, const OutputView& out, uint64_t base, uint32_t row,
+                                           uint32_t c0, bool dense, uint32_t tsize, double* vals, uint32_t* keys) {
+    unsigned long long* vbits = reinterpret_cast<unsigned long long*>(vals);
+    const uint32_t lane = lane_id();
+    uint32_t rt[FA > 0 ? FA : 1];
+    if (FA > 0)
+        for (int m = 0; m < FA; ++m) rt[m] = op.row_tuple[(uint64_t)row * FA + m];
+    uint64_t o = base;
+    for (uint32_t i = 0; i < tsize; i += 128) {
+        bool occ[4];
+        uint32_t col[4];
+        double v[4];
+        uint32_t m[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const uint32_t sidx = i + u * 32 + lane;
+            occ[u] = false;
+            if (i + u * 32 < tsize) {
+                v[u] = vals[sidx];
+                occ[u] = __double_as_longlong(v[u]) != (long long)kNoValue;
+                col[u] = dense ? c0 + sidx : (occ[u] ? keys[sidx] : 0u);
+                if (occ[u]) {
+                    vbits[sidx] = kNoValue;
+                    if (!dense) keys[sidx] = kEmptyCol;
+                }
+            }
+            m[u] = __ballot_sync(kFullMask, occ[u]);
+        }
+        if (base == ~0ull) continue;  // rerun later: nothing written
+        if (FA > 0) {
+            uint32_t ct[4][FB > 0 ? FB : 1];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (occ[u])
+                    for (int k = 0; k < FB; ++k) ct[u][k] = op.col_tuple[(uint64_t)col[u] * FB + k];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (occ[u]) {
+                    const uint64_t e = o + __popc(m[u] & lanemask_lt());
+                    uint32_t* dst = out.idx + e * (FA + FB);
+                    if (FA == 2 && FB == 2) {
+                        __stcs(reinterpret_cast<uint4*>(dst), make_uint4(rt[0], rt[1], ct[u][0], ct[u][1]));
+                    } else if (FA == 1 && FB == 1) {
+                        __stcs(reinterpret_cast<uint2*>(dst), make_uint2(rt[0], ct[u][0]));
+                    } else {
+                        for (int k = 0; k < FA; ++k) dst[k] = rt[k];
+                        for (int k = 0; k < FB; ++k) dst[FA + k] = ct[u][k];
+                    }
+                    __stcs(out.val + e, v[u]);
+                }
+                o += __popc(m[u]);
+            }
+        } else {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (occ[u]) write_entry(op, out, o + __popc(m[u] & lanemask_lt()), row, col[u], v[u]);
+                o += __popc(m[u]);
+            }
+        }
+    }
+}
+
+template <int FA, int FB>
+__global__ void __launch_bounds__(kTaskWarps * 32, kTaskBlocksPerSm)
     warp_task_kernel(Operands op, const PartItem* __restrict__ tasks, uint32_t ntasks, OutputView out,
                      uint32_t* __restrict__ work_counter, uint32_t* __restrict__ overflow) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -345,7 +445,7 @@ __global__ void __launch_bounds__(kTaskWarps * 32, 6)
         const uint32_t tmask = tsize - 1;
         if (dense != dense_layout) {  // values are all empty after an emission; only keys differ
             if (dense) {
-                for (uint32_t i = kTaskSlots + lane; i < kTaskSlots + kTaskSlots / 2; i += 32) vbits[i] = kNoValue;
+                for (uint32_t i = kTaskSlots + lane; i < kTaskDense; i += 32) vbits[i] = kNoValue;
             } else {
                 for (uint32_t i = lane; i < kTaskSlots; i += 32) keys[i] = kEmptyCol;
             }
@@ -373,30 +473,18 @@ __global__ void __launch_bounds__(kTaskWarps * 32, 6)
             const uint32_t incl = warp_inclusive_scan(L);
             const uint32_t excl = incl - L;
             const uint32_t total = __shfl_sync(kFullMask, incl, 31);
+            // software pipeline: the next chunk's fiber entries load while this one is applied
+            Chunk nxt = total > 0 ? load_chunk(op, 0, total, incl, s, excl) : Chunk{0u, kEmptyCol, 0.0};
             for (uint32_t q0 = 0; q0 < total; q0 += 32) {
-                const uint32_t q = q0 + lane;
-                const bool valid = q < total;
-                // source lane: number of lanes whose inclusive end is <= q
-                uint32_t kk = 0;
-#pragma unroll
-                for (uint32_t step = 16; step > 0; step >>= 1) {
-                    const uint32_t e = __shfl_sync(kFullMask, incl, kk + step - 1);
-                    if (e <= q) kk += step;
-                }
-                kk = min(kk, 31u);
-                const uint32_t sk = __shfl_sync(kFullMask, s, kk);
-                const uint32_t ek = __shfl_sync(kFullMask, excl, kk);
-                const double ak = __shfl_sync(kFullMask, a, kk);
-                const uint32_t j = sk + (q - ek);
-                uint32_t col = kEmptyCol;
-                double prod = 0.0;
-                if (valid) {
-                    col = __ldg(op.b_col + j);
-                    prod = __dmul_rn(ak, __ldg(op.b_val + j));
-                }
+                const Chunk cur = nxt;
+                if (q0 + 32 < total) nxt = load_chunk(op, q0 + 32, total, incl, s, excl);
+                const bool valid = cur.col != kEmptyCol;
+                const uint32_t col = cur.col;
+                const double ak = __shfl_sync(kFullMask, a, cur.kk);
+                const double prod = valid ? __dmul_rn(ak, cur.bval) : 0.0;
                 // products of a single A nonzero have distinct columns: no ordering inside the chunk
-                const uint32_t k0 = __shfl_sync(kFullMask, kk, 0);
-                const bool single = __all_sync(kFullMask, !valid || kk == k0);
+                const uint32_t k0 = __shfl_sync(kFullMask, cur.kk, 0);
+                const bool single = __all_sync(kFullMask, !valid || cur.kk == k0);
                 int slot = -1;
                 uint32_t rank = 0;
                 if (dense) {
@@ -409,16 +497,16 @@ __global__ void __launch_bounds__(kTaskWarps * 32, 6)
                 } else {
                     uint32_t leader = lane;
                     if (!single) {
-                        const uint32_t m = __match_any_sync(kFullMask, col);
-                        rank = __popc(m & lanemask_lt());
-                        leader = __ffs(m) - 1;
+                        const uint32_t mm = __match_any_sync(kFullMask, col);
+                        rank = __popc(mm & lanemask_lt());
+                        leader = __ffs(mm) - 1;
                     }
                     if (valid && rank == 0) {
                         uint32_t h = hash32(col) & tmask;
                         for (uint32_t probe = 0; probe < tsize; ++probe) {
-                            const uint32_t cur = keys[h];
-                            if (cur == col) { slot = (int)h; break; }
-                            if (cur == kEmptyCol) {
+                            const uint32_t cv = keys[h];
+                            if (cv == col) { slot = (int)h; break; }
+                            if (cv == kEmptyCol) {
                                 const uint32_t old = atomicCAS(&keys[h], kEmptyCol, col);
                                 if (old == kEmptyCol || old == col) { slot = (int)h; break; }
                             }
@@ -436,8 +524,7 @@ __global__ void __launch_bounds__(kTaskWarps * 32, 6)
             }
         }
 
-        // emit in slot order (column order for a dense task), resetting the table; the entry count
-        // is needed first only to claim an output range
+        // output position: exact, or claimed now that the count is known
         const bool any_bad = __any_sync(kFullMask, bad);
         uint64_t base = it.out_off;
         uint32_t cnt = 0;
@@ -458,19 +545,7 @@ __global__ void __launch_bounds__(kTaskWarps * 32, 6)
             base = ~0ull;
         }
         if (out.item_count && lane == 0) out.item_count[t] = base == ~0ull ? 0u : cnt;
-        uint64_t o = base;
-        for (uint32_t i = 0; i < tsize; i += 32) {
-            const uint32_t sidx = i + lane;
-            const bool occ = vbits[sidx] != kNoValue;
-            const uint32_t m = __ballot_sync(kFullMask, occ);
-            if (occ) {
-                if (base != ~0ull) write_entry(op, out, o + __popc(m & lanemask_lt()), row,
-                                               dense ? c0 + sidx : keys[sidx], vals[sidx]);
-                vbits[sidx] = kNoValue;
-                if (!dense) keys[sidx] = kEmptyCol;
-            }
-            o += __popc(m);
-        }
+        emit_table<FA, FB>(op, out, base, row, c0, dense, tsize, vals, keys);
         __syncwarp();
     }
 }
@@ -480,11 +555,17 @@ void launch_warp_tasks(const Operands& op, const PartItem* tasks, uint32_t ntask
     if (ntasks == 0) return;
     const size_t smem = kTaskWarps * kTaskBytes;
     PTC_CUDA(cudaMemsetAsync(work_counter, 0, sizeof(uint32_t), st));
+    // the single-contraction layouts of the common free-mode counts get their own emission
+    auto kernel = warp_task_kernel<0, 0>;
+    if (!op.row_item && op.fa == 2 && op.fb == 2) kernel = warp_task_kernel<2, 2>;
+    else if (!op.row_item && op.fa == 1 && op.fb == 1) kernel = warp_task_kernel<1, 1>;
+    else if (!op.row_item && op.fa == 1 && op.fb == 2) kernel = warp_task_kernel<1, 2>;
+    else if (!op.row_item && op.fa == 2 && op.fb == 1) kernel = warp_task_kernel<2, 1>;
     int per_sm = 1;
-    PTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, warp_task_kernel, kTaskWarps * 32, smem));
+    PTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kTaskWarps * 32, smem));
     per_sm = per_sm < 1 ? 1 : per_sm;
     const uint32_t grid = (uint32_t)std::min<uint64_t>((ntasks + kTaskWarps - 1) / kTaskWarps, (uint64_t)num_sms * per_sm);
-    warp_task_kernel<<<grid, kTaskWarps * 32, smem, st>>>(op, tasks, ntasks, out, work_counter, overflow);
+    kernel<<<grid, kTaskWarps * 32, smem, st>>>(op, tasks, ntasks, out, work_counter, overflow);
     count_launch();
     PTC_CHECK_LAUNCH();
 }
