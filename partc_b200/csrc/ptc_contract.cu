@@ -821,8 +821,17 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
             launch_row_features(op, pl.big_rows, n_big, pl.row_flops, gp, fx, st);
             pl.pred = ar.alloc<float>(n_big);
             sizer_predict_device(*sizer, fx, n_big, pl.pred, ar);
-            launch_predicted_panel_counts(pl.big_rows, n_big, pl.row_flops, pl.pred, gp, P, pl.log2w, ncols,
-                                          kSizerMargin, panel_cnt, st);
+            const uint32_t* item_cols = nullptr;
+            if (F.batch) {  // each row's columns are its item's
+                std::vector<uint32_t> ic(F.nitems);
+                for (uint32_t i = 0; i < F.nitems; ++i) ic[i] = F.colbase[i + 1] - F.colbase[i];
+                uint32_t* d = ar.alloc<uint32_t>(F.nitems);
+                PTC_CUDA(cudaMemcpyAsync(d, ic.data(), F.nitems * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+                PTC_CUDA(cudaStreamSynchronize(st));
+                item_cols = d;
+            }
+            launch_predicted_panel_counts(pl.big_rows, n_big, pl.row_flops, pl.pred, gp, op.row_item, item_cols, P,
+                                          pl.log2w, ncols, kSizerMargin, panel_cnt, ar);
             launch_claim_budgets(pl.big_rows, n_big, panel_cnt, P, pl.claim_off, st);
         }
         exclusive_scan<uint64_t>(pl.claim_off, pl.claim_off, nrows, ar);

@@ -17,33 +17,68 @@ __device__ __forceinline__ float popularity_at(const float* __restrict__ row, fl
 }
 
 // cnt[i * P + p] = ceil(margin * D_pred(i) * G_p(F_i) / G(F_i)), at most the panel's width and
-// the row's products; D_pred = 2^pred - 1 clamped to [1, min(F, ncols)].
+// the row's products; D_pred = 2^pred - 1 clamped to [1, min(F, ncols)].  In a batch
+// (row_item != null) a row's columns are its item's: panels past the item's item_cols[item]
+// columns get nothing and the shares are taken over the item's panels (cum = the table's prefix
+// sums over panels).
 __global__ void predicted_panel_counts_kernel(const uint32_t* __restrict__ rows, uint64_t n,
                                               const uint64_t* __restrict__ row_flops, const float* __restrict__ pred,
-                                              const float* __restrict__ gp, uint32_t P, uint32_t panel_log2,
+                                              const float* __restrict__ gp, const float* __restrict__ cum,
+                                              const uint32_t* __restrict__ row_item,
+                                              const uint32_t* __restrict__ item_cols, uint32_t P, uint32_t panel_log2,
                                               uint64_t ncols, float margin, uint32_t* __restrict__ cnt) {
     const uint64_t id = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= n * P) return;
     const uint64_t i = id / P;
     const uint32_t p = (uint32_t)(id % P);
     const float F = (float)row_flops[rows[i]];
-    float d = exp2f(pred[i]) - 1.f;
-    d = fminf(fmaxf(d, 1.f), fminf(F, (float)ncols));
-    const float tot = popularity_at(gp + (uint64_t)P * kGridPoints, F);
-    const float share = tot > 0.f ? popularity_at(gp + (uint64_t)p * kGridPoints, F) / tot : 1.f / P;
+    uint64_t nc = ncols;
+    uint32_t Pi = P;
+    if (row_item) {
+        nc = item_cols[row_item[rows[i]]];
+        Pi = (uint32_t)((nc + (1ull << panel_log2) - 1) >> panel_log2);
+    }
     const uint64_t lo = (uint64_t)p << panel_log2;
-    const uint64_t width = (ncols - lo) < (1ull << panel_log2) ? (ncols - lo) : (1ull << panel_log2);
+    if (p >= Pi || lo >= nc) {
+        cnt[id] = 0;
+        return;
+    }
+    float d = exp2f(pred[i]) - 1.f;
+    d = fminf(fmaxf(d, 1.f), fminf(F, (float)nc));
+    const float tot = row_item ? popularity_at(cum + (uint64_t)Pi * kGridPoints, F)
+                               : popularity_at(gp + (uint64_t)P * kGridPoints, F);
+    const float share = tot > 0.f ? popularity_at(gp + (uint64_t)p * kGridPoints, F) / tot : 1.f / Pi;
+    const uint64_t width = (nc - lo) < (1ull << panel_log2) ? (nc - lo) : (1ull << panel_log2);
     float c = ceilf(margin * d * share);
     c = fminf(fminf(c, (float)width), F);
     cnt[id] = (uint32_t)c;
 }
 
+// cum[p * G + g] = sum over panels q < p of gp[q * G + g], p = 0..P
+__global__ void popularity_prefix_kernel(const float* __restrict__ gp, uint32_t P, float* __restrict__ cum) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= kGridPoints) return;
+    float acc = 0.f;
+    for (uint32_t p = 0; p <= P; ++p) {
+        cum[(uint64_t)p * kGridPoints + g] = acc;
+        if (p < P) acc += gp[(uint64_t)p * kGridPoints + g];
+    }
+}
+
 void launch_predicted_panel_counts(const uint32_t* rows, uint64_t n, const uint64_t* row_flops, const float* pred,
-                                   const float* gp, uint32_t P, uint32_t panel_log2, uint64_t ncols, float margin,
-                                   uint32_t* cnt, cudaStream_t st) {
+                                   const float* gp, const uint32_t* row_item, const uint32_t* item_cols, uint32_t P,
+                                   uint32_t panel_log2, uint64_t ncols, float margin, uint32_t* cnt, Arena& ar) {
     if (n == 0) return;
-    predicted_panel_counts_kernel<<<ceil_div_u32(n * P, 256), 256, 0, st>>>(rows, n, row_flops, pred, gp, P,
-                                                                           panel_log2, ncols, margin, cnt);
+    cudaStream_t st = ar.stream();
+    float* cum = nullptr;
+    if (row_item) {
+        cum = ar.alloc<float>((uint64_t)(P + 1) * kGridPoints);
+        popularity_prefix_kernel<<<ceil_div_u32(kGridPoints, 128), 128, 0, st>>>(gp, P, cum);
+        count_launch();
+        PTC_CHECK_LAUNCH();
+    }
+    predicted_panel_counts_kernel<<<ceil_div_u32(n * P, 256), 256, 0, st>>>(
+        rows, n, row_flops, pred, gp, cum, row_item, item_cols, P, panel_log2, ncols, margin, cnt);
     count_launch();
     PTC_CHECK_LAUNCH();
 }
