@@ -400,6 +400,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--path", default="learned", choices=["two_phase", "learned"])
     ap.add_argument("--no-compare-paths", dest="compare_paths", action="store_false")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false")
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-target-flops", type=float, default=6e7)
@@ -471,6 +472,16 @@ def main():
     keep = []
     coo = _lib.device_coo(di.data_ptr(), dv.data_ptr(), t.nnz, t.dims, keep)
     opts = dict(output_location="device", device=local, stream=stream.cuda_stream, path=args.path)
+    knobs = {}
+    if args.autotune:  # the library's autotuner picks the knobs on this workload (untimed)
+        items = (_lib.BatchItem * 1)()
+        items[0].A = coo
+        items[0].c = w.c
+        for j, m in enumerate(w.modes):
+            items[0].a_modes[j] = m
+        knobs, tune = _lib.autotune(items, repeats=1, device=local, stream=stream.cuda_stream, path=args.path)
+        knobs = {k: v for k, v in knobs.items() if v}
+        opts.update(knobs)
 
     def step():
         out, st = _lib.contract_coo(coo, None, w.c, w.modes, **opts)
@@ -547,7 +558,7 @@ def main():
         pi = torch.from_numpy(t.idx.view(np.int32)).pin_memory()
         pv = torch.from_numpy(t.vals).pin_memory()
         ht = CooTensor(idx=pi.numpy().view(np.uint32), vals=pv.numpy(), dims=t.dims)
-        e2e_opts = dict(device=local, stream=stream.cuda_stream, path=args.path)
+        e2e_opts = dict(device=local, stream=stream.cuda_stream, path=args.path, **knobs)
         idx, vals, _ = _lib.contract(ht, None, w.c, w.modes, **e2e_opts)  # warm-up
         del idx, vals
         pdist.barrier()
@@ -577,6 +588,7 @@ def main():
             "data": "synthetic (seeded generator partc_b200/gen.py: per-mode Zipf(1.1), U(0,1) values, seed 1)",
             "config": {"workload": w.name, "nnz": t.nnz, "dims": [int(x) for x in t.dims],
                        "contracted_modes": w.modes[:w.c], "path": args.path, "parallelism": f"replicas x{world}",
+                       "knobs": knobs or "defaults",
                        "mult_adds_per_step": M, "out_nnz_per_step": R,
                        "l2": "no flush needed: each step writes a 41 GB output (>> 126 MB L2)"},
             "hbm_gbs_numeric": achieved,

@@ -555,12 +555,14 @@ void launch_warp_tasks(const Operands& op, const PartItem* tasks, uint32_t ntask
     if (ntasks == 0) return;
     const size_t smem = kTaskWarps * kTaskBytes;
     PTC_CUDA(cudaMemsetAsync(work_counter, 0, sizeof(uint32_t), st));
-    // the single-contraction layouts of the common free-mode counts get their own emission
+    // the single-contraction layouts of the common free-mode counts get their own emission (the
+    // general one also records rows and columns for the canonical order)
     auto kernel = warp_task_kernel<0, 0>;
-    if (!op.row_item && op.fa == 2 && op.fb == 2) kernel = warp_task_kernel<2, 2>;
-    else if (!op.row_item && op.fa == 1 && op.fb == 1) kernel = warp_task_kernel<1, 1>;
-    else if (!op.row_item && op.fa == 1 && op.fb == 2) kernel = warp_task_kernel<1, 2>;
-    else if (!op.row_item && op.fa == 2 && op.fb == 1) kernel = warp_task_kernel<2, 1>;
+    const bool plain = !op.row_item && !out.row_of;
+    if (plain && op.fa == 2 && op.fb == 2) kernel = warp_task_kernel<2, 2>;
+    else if (plain && op.fa == 1 && op.fb == 1) kernel = warp_task_kernel<1, 1>;
+    else if (plain && op.fa == 1 && op.fb == 2) kernel = warp_task_kernel<1, 2>;
+    else if (plain && op.fa == 2 && op.fb == 1) kernel = warp_task_kernel<2, 1>;
     int per_sm = 1;
     PTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kTaskWarps * 32, smem));
     per_sm = per_sm < 1 ? 1 : per_sm;
