@@ -2,8 +2,9 @@
 //
 //     ptc_tc <tensor.tns> <tensor.meta> <isMtx 0/1> <numTests>
 //
-// It reads the tensor (FROSTT text, 1-based, like readTensor in mtxTnsIO.cpp:30-65; or a
-// MatrixMarket coordinate file when isMtx is 1, like readMatrix), reads the meta file like
+// It reads the tensor (FROSTT text, 1-based, on the GPU with ptc_read_tns, which gives what
+// readTensor in mtxTnsIO.cpp:30-65 gives; or a MatrixMarket coordinate file on the host when isMtx
+// is 1, like readMatrix), reads the meta file like
 // Tensor::populate_meta_info (tensor.hpp:151-173), prints the mode sizes like main.cpp:107-109,
 // and replaces main.cpp:112-118 (B = A, both hash tables, tc_fksCuckoo) with one call to
 // ptc_self_contract.  The library prints the reference's timing and nnz lines.
@@ -19,34 +20,6 @@
 #include "partc.h"
 
 namespace {
-
-bool read_tns(const std::string& path, std::vector<uint32_t>& idx, std::vector<double>& vals,
-              std::vector<uint32_t>& dims, uint32_t& d) {
-    std::ifstream in(path);
-    if (!in) return false;
-    std::string line;
-    d = 0;
-    while (std::getline(in, line)) {
-        if (line.empty() || line[0] == '#') continue;
-        std::istringstream ls(line);
-        std::vector<double> tok;
-        double x;
-        while (ls >> x) tok.push_back(x);
-        if (tok.size() < 2) continue;
-        if (d == 0) {
-            d = (uint32_t)tok.size() - 1;
-            dims.assign(d, 0);
-        }
-        if (tok.size() != d + 1) return false;
-        for (uint32_t m = 0; m < d; ++m) {
-            const uint32_t v = (uint32_t)tok[m] - 1;  // 1-based labels -> 0-based indices
-            idx.push_back(v);
-            if (v + 1 > dims[m]) dims[m] = v + 1;  // mode size = largest label
-        }
-        vals.push_back(tok[d]);
-    }
-    return d > 0;
-}
 
 bool read_mtx(const std::string& path, std::vector<uint32_t>& idx, std::vector<double>& vals,
               std::vector<uint32_t>& dims, uint32_t& d) {
@@ -105,7 +78,24 @@ int main(int argc, char** argv) {
     std::vector<uint32_t> idx, dims, dim_tc;
     std::vector<double> vals;
     uint32_t d = 0, c = 0;
-    const bool ok = is_mtx ? read_mtx(file_a, idx, vals, dims, d) : read_tns(file_a, idx, vals, dims, d);
+    ptc_tensor dev_in;  // a .tns file is read on the GPU and stays there
+    std::memset(&dev_in, 0, sizeof(dev_in));
+    bool ok = false;
+    if (is_mtx) {
+        ok = read_mtx(file_a, idx, vals, dims, d);
+    } else {
+        ptc_options ro;
+        ptc_options_init(&ro);
+        ro.output_location = PTC_DEVICE;
+        uint32_t dm[16];
+        ok = ptc_read_tns(file_a.c_str(), &ro, &dev_in, dm) == PTC_OK;
+        if (ok) {
+            d = dev_in.order;
+            dims.assign(dm, dm + d);
+        } else {
+            std::cerr << ptc_last_error() << std::endl;
+        }
+    }
     if (!ok) {
         std::cerr << "Could not read \"" << file_a << "\"" << std::endl;
         return 1;
@@ -122,8 +112,23 @@ int main(int argc, char** argv) {
     opt.verbose = 1;
     ptc_tensor out;
     ptc_stats stats;
-    const ptc_status s = ptc_self_contract(idx.data(), vals.data(), d, vals.size(), dims.data(), c, dim_tc.data(),
-                                           &opt, &out, &stats);
+    ptc_status s;
+    if (is_mtx) {
+        s = ptc_self_contract(idx.data(), vals.data(), d, vals.size(), dims.data(), c, dim_tc.data(), &opt, &out,
+                              &stats);
+    } else {
+        ptc_coo A;
+        A.order = d;
+        A.location = PTC_DEVICE;
+        A.nnz = dev_in.nnz;
+        A.idx = dev_in.idx;
+        A.vals = dev_in.vals;
+        A.dims = dims.data();
+        // the reference's self-contraction rule: B = A needs more than one nonzero
+        s = A.nnz > 1 ? ptc_contract(&A, nullptr, c, dim_tc.data(), dim_tc.data(), &opt, &out, &stats)
+                      : PTC_ERR_TOO_FEW_NONZEROS;
+        ptc_tensor_free(&dev_in);
+    }
     if (s != PTC_OK) {
         std::cerr << ptc_status_string(s) << ": " << ptc_last_error() << std::endl;
         return 1;
