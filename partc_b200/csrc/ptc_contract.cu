@@ -516,7 +516,7 @@ uint64_t learned_reruns(const Operands& op, std::vector<Launched> groups, const 
         uint32_t* cnt = ar.alloc<uint32_t>((uint64_t)nr * P);
         uint64_t* scratch_d = ar.alloc<uint64_t>(nrows);
         PTC_CUDA(cudaMemsetAsync(scratch_d, 0, nrows * sizeof(uint64_t), st));
-        launch_sym_bitmap(op, drows, nr, cnt, scratch_d, work_counter, num_sms, st);
+        launch_sym_bitmap(op, drows, nr, cnt, nullptr, scratch_d, work_counter, num_sms, st);
         uint32_t* np = ar.alloc<uint32_t>((uint64_t)nfail + 1);
         uint32_t* tot = ar.alloc<uint32_t>(nfail);
         launch_count_parts_range(failed, dridx, nfail, cnt, P, rule, np, tot, st);
@@ -714,10 +714,23 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
                 "more than 1.5M distinct B free keys in one contraction is not supported yet");
     auto table_bytes = [&](uint32_t w) { return nfib * ((ncols + w - 1) / w + 1) * 4; };
     uint32_t W = opt.panel_width;
-    if (W == 0) {  // at most 256 columns (a quarter of a dense warp task), wider for small tables
+    // a batch's large rows each have their own item's panels: per-row panel counts
+    std::vector<uint32_t> item_cols_h;
+    if (F.batch) {
+        item_cols_h.resize(F.nitems);
+        for (uint32_t i = 0; i < F.nitems; ++i) item_cols_h[i] = F.colbase[i + 1] - F.colbase[i];
+    }
+    auto panel_entries = [&](uint32_t w) {  // panel counters of the large rows (an upper bound for a batch)
+        if (!F.batch) return (uint64_t)n_big * ((ncols + w - 1) / w);
+        uint64_t e = 0;
+        for (uint32_t i = 0; i < F.nitems; ++i)
+            e += (uint64_t)(F.h_row_first[i + 1] - F.h_row_first[i]) * std::max<uint64_t>(1, (item_cols_h[i] + w - 1) / w);
+        return e;
+    };
+    if (W == 0) {  // at most 256 columns (a third of a dense warp task), wider for small tables
         W = 32;
         while (W < 256 && (uint64_t)W * 16 < ncols) W <<= 1;
-        while (W < warp_task_dense_columns() && (uint64_t)n_big * ((ncols + W - 1) / W) * 4 > (2ull << 30)) W <<= 1;
+        while (W < warp_task_dense_columns() && panel_entries(W) * 4 > (2ull << 30)) W <<= 1;
     }
     PTC_REQUIRE(W <= hash_part_capacity(), PTC_ERR_INVALID_ARGUMENT, "panel_width larger than a hash part");
     pl.W = W;
@@ -762,11 +775,25 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
     // panel; two-phase path only -- the learned path predicts those)
     uint64_t* row_d = ar.alloc<uint64_t>(nrows + 1);
     PTC_CUDA(cudaMemsetAsync(row_d, 0, (nrows + 1) * sizeof(uint64_t), st));
-    uint32_t* panel_cnt = ar.alloc<uint32_t>((uint64_t)n_big * P);
+    const uint64_t* pbase = nullptr;  // per-row panel offsets (batches; null: row i at i * P)
+    const uint32_t* item_cols = nullptr;
+    uint64_t n_panel_cnt = (uint64_t)n_big * P;
+    if (F.batch) {
+        uint32_t* ic = ar.alloc<uint32_t>(F.nitems);
+        PTC_CUDA(cudaMemcpyAsync(ic, item_cols_h.data(), F.nitems * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        item_cols = ic;
+        uint64_t* pb = ar.alloc<uint64_t>((uint64_t)n_big + 1);
+        launch_row_panel_counts(pl.big_rows, n_big, op.row_item, item_cols, pl.log2w, pb, st);
+        exclusive_scan<uint64_t>(pb, pb, n_big, ar);
+        n_panel_cnt = read_scalar(pb + n_big, st);  // also orders the copy of item_cols_h
+        pbase = pb;
+    }
+    uint32_t* panel_cnt = ar.alloc<uint32_t>(std::max<uint64_t>(n_panel_cnt, 1));
     pl.work_counter = ar.alloc<uint32_t>(1);
     OutputView none;
     launch_small_rows(false, op, pl.small_rows, n_small, row_d, nullptr, none, st);
-    if (!pl.learned) launch_sym_bitmap(op, pl.big_rows, n_big, panel_cnt, row_d, pl.work_counter, num_sms, st);
+    if (!pl.learned)
+        launch_sym_bitmap(op, pl.big_rows, n_big, panel_cnt, pbase, row_d, pl.work_counter, num_sms, st);
     // sort-based rows: expand their products in stream order, sort stably by (row, column)
     pl.esc_colbits = (uint32_t)colbits;
     if (n_esc > 0) {
@@ -821,18 +848,9 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
             launch_row_features(op, pl.big_rows, n_big, pl.row_flops, gp, fx, st);
             pl.pred = ar.alloc<float>(n_big);
             sizer_predict_device(*sizer, fx, n_big, pl.pred, ar);
-            const uint32_t* item_cols = nullptr;
-            if (F.batch) {  // each row's columns are its item's
-                std::vector<uint32_t> ic(F.nitems);
-                for (uint32_t i = 0; i < F.nitems; ++i) ic[i] = F.colbase[i + 1] - F.colbase[i];
-                uint32_t* d = ar.alloc<uint32_t>(F.nitems);
-                PTC_CUDA(cudaMemcpyAsync(d, ic.data(), F.nitems * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-                PTC_CUDA(cudaStreamSynchronize(st));
-                item_cols = d;
-            }
-            launch_predicted_panel_counts(pl.big_rows, n_big, pl.row_flops, pl.pred, gp, op.row_item, item_cols, P,
-                                          pl.log2w, ncols, kSizerMargin, panel_cnt, ar);
-            launch_claim_budgets(pl.big_rows, n_big, panel_cnt, P, pl.claim_off, st);
+            launch_predicted_panel_counts(pl.big_rows, n_big, pl.row_flops, pl.pred, gp, op.row_item, item_cols,
+                                          pbase, P, pl.log2w, ncols, kSizerMargin, panel_cnt, ar);
+            launch_claim_budgets(pl.big_rows, n_big, panel_cnt, pbase, P, pl.claim_off, st);
         }
         exclusive_scan<uint64_t>(pl.claim_off, pl.claim_off, nrows, ar);
         pl.claim_total = read_scalar(pl.claim_off + nrows, st);
@@ -842,13 +860,15 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
     for (int kind = 0; kind < 2; ++kind) {
         const uint64_t r0 = kind == 0 ? 0 : pl.n_warp_rows, nr = kind == 0 ? pl.n_warp_rows : n_big - pl.n_warp_rows;
         uint32_t* nparts = ar.alloc<uint32_t>(nr + 1);
-        launch_count_parts(panel_cnt + r0 * P, nr, P, pl.rule[kind], nparts, op.err, st);
+        const uint32_t* pc = pbase ? panel_cnt : panel_cnt + r0 * P;
+        const uint64_t* pb = pbase ? pbase + r0 : nullptr;
+        launch_count_parts(pc, pb, nr, P, pl.rule[kind], nparts, op.err, st);
         exclusive_scan<uint32_t>(nparts, nparts, nr, ar);
         pl.n_parts[kind] = read_scalar(nparts + nr, st);
         PTC_REQUIRE(read_scalar(op.err, st) == 0, PTC_ERR_INTERNAL, "a fine panel exceeds the hash part capacity");
         pl.parts[kind] = ar.alloc<PartItem>(pl.n_parts[kind]);
-        launch_fill_parts(pl.big_rows + r0, panel_cnt + r0 * P, nr, P, pl.rule[kind], nparts,
-                          pl.learned ? nullptr : pl.row_off, pl.parts[kind], st);
+        launch_fill_parts(pl.big_rows + r0, pc, pb, nr, P, pl.rule[kind], nparts, pl.learned ? nullptr : pl.row_off,
+                          pl.parts[kind], st);
     }
     stats.hash_parts = pl.n_parts[0] + pl.n_parts[1];
     return pl;

@@ -25,33 +25,31 @@ __global__ void predicted_panel_counts_kernel(const uint32_t* __restrict__ rows,
                                               const uint64_t* __restrict__ row_flops, const float* __restrict__ pred,
                                               const float* __restrict__ gp, const float* __restrict__ cum,
                                               const uint32_t* __restrict__ row_item,
-                                              const uint32_t* __restrict__ item_cols, uint32_t P, uint32_t panel_log2,
+                                              const uint32_t* __restrict__ item_cols,
+                                              const uint64_t* __restrict__ pbase, uint32_t P, uint32_t panel_log2,
                                               uint64_t ncols, float margin, uint32_t* __restrict__ cnt) {
-    const uint64_t id = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= n * P) return;
-    const uint64_t i = id / P;
-    const uint32_t p = (uint32_t)(id % P);
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
     const float F = (float)row_flops[rows[i]];
-    uint64_t nc = ncols;
-    uint32_t Pi = P;
-    if (row_item) {
-        nc = item_cols[row_item[rows[i]]];
-        Pi = (uint32_t)((nc + (1ull << panel_log2) - 1) >> panel_log2);
-    }
-    const uint64_t lo = (uint64_t)p << panel_log2;
-    if (p >= Pi || lo >= nc) {
-        cnt[id] = 0;
-        return;
-    }
+    const uint64_t nc = row_item ? item_cols[row_item[rows[i]]] : ncols;
+    const uint64_t base = pbase ? pbase[i] : i * P;
+    const uint32_t Pi = pbase ? (uint32_t)(pbase[i + 1] - pbase[i]) : P;
     float d = exp2f(pred[i]) - 1.f;
     d = fminf(fmaxf(d, 1.f), fminf(F, (float)nc));
     const float tot = row_item ? popularity_at(cum + (uint64_t)Pi * kGridPoints, F)
                                : popularity_at(gp + (uint64_t)P * kGridPoints, F);
-    const float share = tot > 0.f ? popularity_at(gp + (uint64_t)p * kGridPoints, F) / tot : 1.f / Pi;
-    const uint64_t width = (nc - lo) < (1ull << panel_log2) ? (nc - lo) : (1ull << panel_log2);
-    float c = ceilf(margin * d * share);
-    c = fminf(fminf(c, (float)width), F);
-    cnt[id] = (uint32_t)c;
+    for (uint32_t p = 0; p < Pi; ++p) {
+        const uint64_t lo = (uint64_t)p << panel_log2;
+        if (lo >= nc) {
+            cnt[base + p] = 0;
+            continue;
+        }
+        const float share = tot > 0.f ? popularity_at(gp + (uint64_t)p * kGridPoints, F) / tot : 1.f / Pi;
+        const uint64_t width = (nc - lo) < (1ull << panel_log2) ? (nc - lo) : (1ull << panel_log2);
+        float c = ceilf(margin * d * share);
+        c = fminf(fminf(c, (float)width), F);
+        cnt[base + p] = (uint32_t)c;
+    }
 }
 
 // cum[p * G + g] = sum over panels q < p of gp[q * G + g], p = 0..P
@@ -66,8 +64,9 @@ __global__ void popularity_prefix_kernel(const float* __restrict__ gp, uint32_t 
 }
 
 void launch_predicted_panel_counts(const uint32_t* rows, uint64_t n, const uint64_t* row_flops, const float* pred,
-                                   const float* gp, const uint32_t* row_item, const uint32_t* item_cols, uint32_t P,
-                                   uint32_t panel_log2, uint64_t ncols, float margin, uint32_t* cnt, Arena& ar) {
+                                   const float* gp, const uint32_t* row_item, const uint32_t* item_cols,
+                                   const uint64_t* pbase, uint32_t P, uint32_t panel_log2, uint64_t ncols, float margin,
+                                   uint32_t* cnt, Arena& ar) {
     if (n == 0) return;
     cudaStream_t st = ar.stream();
     float* cum = nullptr;
@@ -77,8 +76,8 @@ void launch_predicted_panel_counts(const uint32_t* rows, uint64_t n, const uint6
         count_launch();
         PTC_CHECK_LAUNCH();
     }
-    predicted_panel_counts_kernel<<<ceil_div_u32(n * P, 256), 256, 0, st>>>(
-        rows, n, row_flops, pred, gp, cum, row_item, item_cols, P, panel_log2, ncols, margin, cnt);
+    predicted_panel_counts_kernel<<<ceil_div_u32(n, 128), 128, 0, st>>>(
+        rows, n, row_flops, pred, gp, cum, row_item, item_cols, pbase, P, panel_log2, ncols, margin, cnt);
     count_launch();
     PTC_CHECK_LAUNCH();
 }
@@ -152,18 +151,19 @@ void launch_log2_error(const uint32_t* rows, uint64_t n, const float* pred, cons
 
 // budget[rows[i]] = sum of the row's predicted panel counts (the budgets of its parts)
 __global__ void big_budget_kernel(const uint32_t* __restrict__ rows, uint64_t n, const uint32_t* __restrict__ cnt,
-                                  uint32_t P, uint64_t* __restrict__ budget) {
+                                  const uint64_t* __restrict__ pbase, uint32_t P, uint64_t* __restrict__ budget) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const uint64_t b = pbase ? pbase[i] : i * P, e = pbase ? pbase[i + 1] : (i + 1) * P;
     uint64_t s = 0;
-    for (uint32_t p = 0; p < P; ++p) s += cnt[i * P + p];
+    for (uint64_t p = b; p < e; ++p) s += cnt[p];
     budget[rows[i]] = s;
 }
 
-void launch_claim_budgets(const uint32_t* big_rows, uint64_t n_big, const uint32_t* panel_cnt, uint32_t P,
-                          uint64_t* budget, cudaStream_t st) {
+void launch_claim_budgets(const uint32_t* big_rows, uint64_t n_big, const uint32_t* panel_cnt, const uint64_t* pbase,
+                          uint32_t P, uint64_t* budget, cudaStream_t st) {
     if (n_big == 0) return;
-    big_budget_kernel<<<ceil_div_u32(n_big, 256), 256, 0, st>>>(big_rows, n_big, panel_cnt, P, budget);
+    big_budget_kernel<<<ceil_div_u32(n_big, 256), 256, 0, st>>>(big_rows, n_big, panel_cnt, pbase, P, budget);
     count_launch();
     PTC_CHECK_LAUNCH();
 }

@@ -128,33 +128,48 @@ __device__ __forceinline__ uint32_t split_panels(const uint32_t* cnt, uint32_t P
     return parts;
 }
 
-__global__ void count_parts_kernel(const uint32_t* __restrict__ panel_cnt, uint64_t nbig, uint32_t P, SplitRule rule,
-                                   uint32_t* __restrict__ nparts, uint32_t* __restrict__ oversize) {
+// Panels of large row i: [pbase[i], pbase[i + 1]) of panel_cnt, or i * P + [0, P) without pbase.
+__device__ __forceinline__ void row_panels(const uint64_t* pbase, uint64_t i, uint32_t P, uint64_t& base, uint32_t& n) {
+    base = pbase ? pbase[i] : i * P;
+    n = pbase ? (uint32_t)(pbase[i + 1] - pbase[i]) : P;
+}
+
+__global__ void count_parts_kernel(const uint32_t* __restrict__ panel_cnt, const uint64_t* __restrict__ pbase,
+                                   uint64_t nbig, uint32_t P, SplitRule rule, uint32_t* __restrict__ nparts,
+                                   uint32_t* __restrict__ oversize) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nbig) return;
+    uint64_t b;
+    uint32_t n;
+    row_panels(pbase, i, P, b, n);
     bool over = false;
-    nparts[i] = split_panels(panel_cnt + i * P, P, rule, &over, [](uint32_t, uint32_t, uint64_t, uint32_t) {});
+    nparts[i] = split_panels(panel_cnt + b, n, rule, &over, [](uint32_t, uint32_t, uint64_t, uint32_t) {});
     if (over) atomicOr(oversize, 1u);
 }
 
-void launch_count_parts(const uint32_t* panel_cnt, uint64_t nbig, uint32_t npanels, SplitRule rule, uint32_t* nparts,
-                        uint32_t* oversize, cudaStream_t st) {
+void launch_count_parts(const uint32_t* panel_cnt, const uint64_t* pbase, uint64_t nbig, uint32_t npanels,
+                        SplitRule rule, uint32_t* nparts, uint32_t* oversize, cudaStream_t st) {
     if (nbig == 0) return;
-    count_parts_kernel<<<ceil_div_u32(nbig, 256), 256, 0, st>>>(panel_cnt, nbig, npanels, rule, nparts, oversize);
+    count_parts_kernel<<<ceil_div_u32(nbig, 256), 256, 0, st>>>(panel_cnt, pbase, nbig, npanels, rule, nparts,
+                                                                oversize);
     count_launch();
     PTC_CHECK_LAUNCH();
 }
 
 __global__ void fill_parts_kernel(const uint32_t* __restrict__ rows, const uint32_t* __restrict__ panel_cnt,
-                                  uint64_t nbig, uint32_t P, SplitRule rule, const uint32_t* __restrict__ part_pos,
-                                  const uint64_t* __restrict__ row_off, PartItem* __restrict__ parts) {
+                                  const uint64_t* __restrict__ pbase, uint64_t nbig, uint32_t P, SplitRule rule,
+                                  const uint32_t* __restrict__ part_pos, const uint64_t* __restrict__ row_off,
+                                  PartItem* __restrict__ parts) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nbig) return;
     const uint32_t row = rows[i];
     const uint64_t base = row_off ? row_off[row] : 0;  // no offsets: the parts claim output later
+    uint64_t b;
+    uint32_t n;
+    row_panels(pbase, i, P, b, n);
     uint32_t o = part_pos[i];
     bool over = false;
-    split_panels(panel_cnt + i * P, P, rule, &over, [&](uint32_t p0, uint32_t p1, uint64_t before, uint32_t mode) {
+    split_panels(panel_cnt + b, n, rule, &over, [&](uint32_t p0, uint32_t p1, uint64_t before, uint32_t mode) {
         PartItem it;
         it.row = row;
         it.p0 = p0;
@@ -165,11 +180,30 @@ __global__ void fill_parts_kernel(const uint32_t* __restrict__ rows, const uint3
     });
 }
 
-void launch_fill_parts(const uint32_t* rows, const uint32_t* panel_cnt, uint64_t nbig, uint32_t npanels, SplitRule rule,
-                       const uint32_t* part_pos, const uint64_t* row_off, PartItem* parts, cudaStream_t st) {
+void launch_fill_parts(const uint32_t* rows, const uint32_t* panel_cnt, const uint64_t* pbase, uint64_t nbig,
+                       uint32_t npanels, SplitRule rule, const uint32_t* part_pos, const uint64_t* row_off,
+                       PartItem* parts, cudaStream_t st) {
     if (nbig == 0) return;
-    fill_parts_kernel<<<ceil_div_u32(nbig, 256), 256, 0, st>>>(rows, panel_cnt, nbig, npanels, rule, part_pos, row_off,
-                                                               parts);
+    fill_parts_kernel<<<ceil_div_u32(nbig, 256), 256, 0, st>>>(rows, panel_cnt, pbase, nbig, npanels, rule, part_pos,
+                                                               row_off, parts);
+    count_launch();
+    PTC_CHECK_LAUNCH();
+}
+
+// panels of every large row of a batch: its item's columns in panels of 2^log2w (at least one)
+__global__ void row_panel_counts_kernel(const uint32_t* __restrict__ rows, uint64_t n,
+                                        const uint32_t* __restrict__ row_item, const uint32_t* __restrict__ item_cols,
+                                        uint32_t log2w, uint64_t* __restrict__ np) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint64_t c = item_cols[row_item[rows[i]]];
+    np[i] = c ? (c + (1ull << log2w) - 1) >> log2w : 1;
+}
+
+void launch_row_panel_counts(const uint32_t* rows, uint64_t n, const uint32_t* row_item, const uint32_t* item_cols,
+                             uint32_t log2w, uint64_t* np, cudaStream_t st) {
+    if (n == 0) return;
+    row_panel_counts_kernel<<<ceil_div_u32(n, 256), 256, 0, st>>>(rows, n, row_item, item_cols, log2w, np);
     count_launch();
     PTC_CHECK_LAUNCH();
 }

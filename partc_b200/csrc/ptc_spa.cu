@@ -201,7 +201,8 @@ constexpr int kSymItems = 4;
 
 __global__ void __launch_bounds__(kSymThreads)
     sym_bitmap_kernel(Operands op, const uint32_t* __restrict__ rows, uint32_t nrows, uint32_t* __restrict__ panel_cnt,
-                      uint64_t* __restrict__ row_d, uint32_t* __restrict__ work_counter, uint32_t nwords) {
+                      const uint64_t* __restrict__ pbase, uint64_t* __restrict__ row_d,
+                      uint32_t* __restrict__ work_counter, uint32_t nwords) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint32_t* bits = reinterpret_cast<uint32_t*>(smem);   // [nwords]
     uint32_t* pc = bits + nwords;                         // [npanels]
@@ -266,13 +267,17 @@ __global__ void __launch_bounds__(kSymThreads)
             __syncthreads();
         }
         uint32_t dsum = 0;
-        for (uint32_t p = t; p < P; p += kSymThreads) {
+        const uint64_t pb = pbase ? pbase[item] : (uint64_t)item * P;
+        const uint32_t pn = pbase ? (uint32_t)(pbase[item + 1] - pbase[item]) : P;  // the row's item's panels
+        // a row's columns lie in its item's panels: only those counters and bitmap words were set
+        for (uint32_t p = t; p < pn; p += kSymThreads) {
             const uint32_t v = pc[p];
-            panel_cnt[(uint64_t)item * P + p] = v;
+            panel_cnt[pb + p] = v;
             dsum += v;
             pc[p] = 0;
         }
-        for (uint32_t i = t; i < nwords; i += kSymThreads) bits[i] = 0;
+        const uint32_t rw = (uint32_t)min((uint64_t)nwords, (((uint64_t)pn << op.panel_log2) + 31) / 32);
+        for (uint32_t i = t; i < rw; i += kSymThreads) bits[i] = 0;
         dsum = warp_sum(dsum);
         if (lane_id() == 0 && dsum) atomicAdd(reinterpret_cast<unsigned long long*>(&row_d[row]), (unsigned long long)dsum);
     }
@@ -280,7 +285,8 @@ __global__ void __launch_bounds__(kSymThreads)
 
 uint32_t sym_bitmap_max_cols() { return 1536u * 1024u; }  // 192 KiB of bitmap
 
-void launch_sym_bitmap(const Operands& op, const uint32_t* rows, uint32_t nrows, uint32_t* panel_cnt, uint64_t* row_d,
+void launch_sym_bitmap(const Operands& op, const uint32_t* rows, uint32_t nrows, uint32_t* panel_cnt,
+                       const uint64_t* pbase, uint64_t* row_d,
                        uint32_t* work_counter, int num_sms, cudaStream_t st) {
     if (nrows == 0) return;
     const uint32_t nwords = (uint32_t)((op.ncols + 31) / 32);
@@ -291,7 +297,8 @@ void launch_sym_bitmap(const Operands& op, const uint32_t* rows, uint32_t nrows,
     PTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sym_bitmap_kernel, kSymThreads, smem));
     per_sm = per_sm < 1 ? 1 : per_sm;
     const uint32_t grid = (uint32_t)std::min<uint64_t>(nrows, (uint64_t)num_sms * per_sm);
-    sym_bitmap_kernel<<<grid, kSymThreads, smem, st>>>(op, rows, nrows, panel_cnt, row_d, work_counter, nwords);
+    sym_bitmap_kernel<<<grid, kSymThreads, smem, st>>>(op, rows, nrows, panel_cnt, pbase, row_d, work_counter,
+                                                         nwords);
     count_launch();
     PTC_CHECK_LAUNCH();
 }

@@ -20,10 +20,10 @@ uint32_t sym_bitmap_max_cols();
 void launch_small_rows(bool numeric, const Operands& op, const uint32_t* rows, uint32_t nrows, uint64_t* row_d,
                        const uint64_t* row_off, const OutputView& out, cudaStream_t st);
 
-// other rows, symbolic: panel_cnt[i * npanels + p] = output nnz of rows[i] in fine panel p;
-// row_d[rows[i]] += the row's total (row_d must start at 0 for these rows)
-void launch_sym_bitmap(const Operands& op, const uint32_t* rows, uint32_t nrows, uint32_t* panel_cnt, uint64_t* row_d,
-                       uint32_t* work_counter, int num_sms, cudaStream_t st);
+// other rows, symbolic: panel_cnt[pbase[i] + p] (pbase null: i * npanels + p) = output nnz of
+// rows[i] in fine panel p; row_d[rows[i]] += the row's total (row_d must start at 0 for these rows)
+void launch_sym_bitmap(const Operands& op, const uint32_t* rows, uint32_t nrows, uint32_t* panel_cnt,
+                       const uint64_t* pbase, uint64_t* row_d, uint32_t* work_counter, int num_sms, cudaStream_t st);
 
 // largest exact output count of a sparse warp task, and its table bounds (log2 slots)
 uint32_t warp_task_capacity();
@@ -85,10 +85,15 @@ struct SplitRule {
     uint32_t oversize_dense;  // 1: a single panel above cap becomes a dense part (else an error)
     uint32_t load_num, load_den;  // open-addressing tables at most load_num / load_den full
 };
-// number of parts of each big row; sets *oversize if one fine panel alone exceeds cap
-void launch_count_parts(const uint32_t* panel_cnt, uint64_t nbig, uint32_t npanels, SplitRule rule, uint32_t* nparts,
-                        uint32_t* oversize, cudaStream_t st);
-void launch_fill_parts(const uint32_t* rows, const uint32_t* panel_cnt, uint64_t nbig, uint32_t npanels, SplitRule rule,
-                       const uint32_t* part_pos, const uint64_t* row_off, PartItem* parts, cudaStream_t st);
+// number of parts of each big row; sets *oversize if one fine panel alone exceeds cap.  Row i's
+// panel counts are panel_cnt[pbase[i] .. pbase[i+1]), or panel_cnt[i * npanels ..] with pbase null.
+void launch_count_parts(const uint32_t* panel_cnt, const uint64_t* pbase, uint64_t nbig, uint32_t npanels,
+                        SplitRule rule, uint32_t* nparts, uint32_t* oversize, cudaStream_t st);
+void launch_fill_parts(const uint32_t* rows, const uint32_t* panel_cnt, const uint64_t* pbase, uint64_t nbig,
+                       uint32_t npanels, SplitRule rule, const uint32_t* part_pos, const uint64_t* row_off,
+                       PartItem* parts, cudaStream_t st);
+// np[i] = panels of rows[i]'s item (a batch): ceil(item_cols[row_item[row]] / 2^log2w), at least 1
+void launch_row_panel_counts(const uint32_t* rows, uint64_t n, const uint32_t* row_item, const uint32_t* item_cols,
+                             uint32_t log2w, uint64_t* np, cudaStream_t st);
 
 }  // namespace ptc
