@@ -161,6 +161,13 @@ def zipf4d_3m(seed: int = 1, nnz: int = 3_100_000) -> Workload:
     return Workload("zipf4d_2482x2862x14036x17_3.1m", t, 2, [0, 1, 2, 3])
 
 
+def zipf4d_500k(seed: int = 1) -> Workload:
+    """The 4-D Zipf workload at 500k nonzeros (same shape, distributions and contraction): the
+    small case for profiler captures."""
+    w = zipf4d_3m(seed=seed, nnz=500_000)
+    return Workload("zipf4d_2482x2862x14036x17_500k", w.tensor, w.c, w.modes)
+
+
 def skew3d_20m(seed: int = 2, nnz: int = 20_000_000) -> Workload:
     """3-D 12000x9000x28000, Zipf(1.3) on mode 1, uniform modes 0 and 2, N(0,1) values,
     contract modes {0,2} (output indexed by mode 1 x mode 1)."""
@@ -171,6 +178,7 @@ def skew3d_20m(seed: int = 2, nnz: int = 20_000_000) -> Workload:
 WORKLOADS = {
     "uniform3d_50k": uniform3d_50k,
     "zipf4d_3m": zipf4d_3m,
+    "zipf4d_500k": zipf4d_500k,
     "skew3d_20m": skew3d_20m,
 }
 
