@@ -128,10 +128,23 @@ __global__ void parse_lines_kernel(const char* __restrict__ buf, uint64_t n, con
         return;
     }
     keep[r] = 1;
+    {  // a data line holds d labels and one value
+        uint32_t tokens = 0;
+        bool in = false;
+        for (const char* x = q; x < e && *x != '\n'; ++x) {
+            const bool sp = *x == ' ' || *x == '\t' || *x == '\r';
+            if (!sp && !in) ++tokens;
+            in = !sp;
+        }
+        if (tokens != d + 1) {
+            atomicOr(err, 1u);
+            return;
+        }
+    }
     for (uint32_t m = 0; m < d; ++m) {
         while (q < e && !is_digit(*q) && *q != '\n') ++q;
         if (q >= e || !is_digit(*q)) {
-            atomicOr(err, 1u);  // fewer labels than the first line
+            atomicOr(err, 1u);  // a label that is not a number
             return;
         }
         uint64_t v = 0;
@@ -256,7 +269,8 @@ extern "C" ptc_status ptc_read_tns(const char* path, const ptc_options* opt_in, 
         uint32_t nnz = 0;
         PTC_CUDA(cudaMemcpyAsync(&nnz, pos + nlines, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         PTC_CUDA(cudaStreamSynchronize(st));
-        PTC_REQUIRE((herr & 1u) == 0, PTC_ERR_INVALID_ARGUMENT, "a line has fewer labels than the first data line");
+        PTC_REQUIRE((herr & 1u) == 0, PTC_ERR_INVALID_ARGUMENT,
+                    "a data line does not hold as many labels as the first one, plus a value");
         PTC_REQUIRE((herr & 2u) == 0, PTC_ERR_INDEX_RANGE, "a label is 0 or does not fit 32 bits (labels are 1-based)");
         uint32_t* dims = ar.alloc<uint32_t>(16);
         PTC_CUDA(cudaMemsetAsync(dims, 0, 16 * sizeof(uint32_t), st));
