@@ -96,14 +96,14 @@ typedef struct ptc_options {
                                   of device memory per output entry); single contractions only */
     /* tuning knobs (0 = default) */
     uint32_t small_max_products;    /* rows with at most this many products use the one-warp
-                                       accumulator (<= 512; default 512) */
+                                       accumulator (<= 512; default 128) */
     uint32_t sort_max_avg_products; /* rows averaging fewer products per A nonzero use the
-                                       sort-based accumulator (default 32) */
+                                       sort-based accumulator (default 64) */
     uint32_t hash_load_pct;         /* cuckoo table load factor in percent, 10-90 (default 75) */
     uint32_t batch_wave_mib;        /* ptc_batch_contract: device memory for one wave's outputs,
                                        MiB (default: 60% of the free memory) */
     uint32_t warp_task_max_len;     /* large rows with at most this many A nonzeros use one warp per
-                                       column range, longer ones one block per part (default 4096) */
+                                       column range, longer ones one block per part (default 1024) */
     uint32_t reserved[2];
 } ptc_options;
 

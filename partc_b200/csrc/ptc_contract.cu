@@ -37,7 +37,9 @@ void set_last_error(ptc_status, const std::string& msg) { g_last_error = msg; }
 namespace {
 
 // rows averaging fewer products per A nonzero than this use the sort-based accumulator
-constexpr uint32_t kEscMaxAvgProducts = 32;
+constexpr uint32_t kEscMaxAvgProducts = 64;
+// rows with at most this many products use the one-warp accumulator (its table holds 512)
+constexpr uint32_t kSmallMaxProducts = 128;
 // a window of fine panels at least 1/kDenseMinFraction full becomes a dense part
 constexpr uint32_t kDenseMinFraction = 5;
 // largest product count the sort-based accumulator buffers (32 bytes per product)
@@ -580,8 +582,7 @@ struct Knobs {
 
 Knobs knobs_of(const ptc_options& opt) {
     Knobs k;
-    k.small_max = opt.small_max_products ? std::min(opt.small_max_products, small_row_max_flops())
-                                         : small_row_max_flops();
+    k.small_max = std::min(opt.small_max_products ? opt.small_max_products : kSmallMaxProducts, small_row_max_flops());
     k.esc_avg = opt.sort_max_avg_products ? opt.sort_max_avg_products : kEscMaxAvgProducts;
     k.max_load = opt.hash_load_pct ? std::min(std::max(opt.hash_load_pct, 10u), 90u) / 100.0 : 0.75;
     return k;
@@ -1927,9 +1928,9 @@ ptc_status ptc_autotune(const ptc_batch_item* items, uint32_t n, const ptc_optio
         };
         const std::vector<Knob> knobs = {
             {&ptc_options::panel_width, {0, 64, 128, 256, 512, 1024}},
-            {&ptc_options::warp_task_max_len, {0, 1024, 16384}},
-            {&ptc_options::small_max_products, {0, 128, 256}},
-            {&ptc_options::sort_max_avg_products, {0, 8, 16, 64}},
+            {&ptc_options::warp_task_max_len, {0, 256, 4096, 16384}},
+            {&ptc_options::small_max_products, {0, 64, 256, 512}},
+            {&ptc_options::sort_max_avg_products, {0, 16, 32, 128}},
             {&ptc_options::hash_load_pct, {0, 50, 90}},
         };
         const uint32_t user_panel = opt.panel_width;
