@@ -152,27 +152,30 @@ void launch_row_flops(const uint64_t* poff, const uint32_t* row_start, uint64_t 
 
 // Dense-panel split of every fiber (B sorted by fiber, then column):
 // off[f * (P + 1) + p] = first entry j of fiber f with b_col[j] >= p << log2w (fiber end if none).
-// One thread per B entry writes the panel boundaries that fall just before it; the last entry of
-// a fiber also writes the boundaries past its column.
-__global__ void panel_offsets_kernel(const uint32_t* __restrict__ b_col, const uint32_t* __restrict__ b_fib,
-                                     const uint32_t* __restrict__ fib_start, uint64_t nb, uint32_t P,
-                                     uint32_t log2w, uint32_t* __restrict__ off) {
-    const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= nb) return;
-    const uint32_t f = b_fib[j];
-    const uint32_t fs = fib_start[f], fe = fib_start[f + 1];
-    const uint32_t q = b_col[j] >> log2w;
-    const int64_t qprev = (j == fs) ? -1 : (int64_t)(b_col[j - 1] >> log2w);
-    uint32_t* o = off + (uint64_t)f * (P + 1);
-    for (int64_t p = qprev + 1; p <= (int64_t)q; ++p) o[p] = (uint32_t)j;
-    if (j + 1 == fe)
-        for (uint32_t p = q + 1; p <= P; ++p) o[p] = fe;
+// One thread per table entry (consecutive threads write consecutive entries): a binary search in
+// the fiber, whose columns the neighbouring threads read too.
+__global__ void panel_offsets_kernel(const uint32_t* __restrict__ b_col, const uint32_t* __restrict__ fib_start,
+                                     uint64_t nfib, uint32_t P, uint32_t log2w, uint32_t* __restrict__ off) {
+    const uint64_t n = nfib * (P + 1);
+    for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < n; x += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t f = x / (P + 1);
+        const uint32_t p = (uint32_t)(x - f * (P + 1));
+        uint32_t lo = fib_start[f], hi = fib_start[f + 1];
+        const uint64_t c = (uint64_t)p << log2w;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (b_col[mid] < c) lo = mid + 1; else hi = mid;
+        }
+        off[x] = lo;
+    }
 }
 
-void launch_panel_offsets(const uint32_t* b_col, const uint32_t* b_fib, const uint32_t* fib_start, uint64_t nb,
-                          uint32_t P, uint32_t log2w, uint32_t* off, cudaStream_t st) {
-    if (nb == 0) return;
-    panel_offsets_kernel<<<ceil_div_u32(nb, 256), 256, 0, st>>>(b_col, b_fib, fib_start, nb, P, log2w, off);
+void launch_panel_offsets(const uint32_t* b_col, const uint32_t* fib_start, uint64_t nfib, uint32_t P, uint32_t log2w,
+                          uint32_t* off, cudaStream_t st) {
+    if (nfib == 0) return;
+    const uint64_t n = nfib * (P + 1);
+    const uint32_t grid = (uint32_t)std::min<uint64_t>((n + 255) / 256, 148ull * 64);
+    panel_offsets_kernel<<<grid, 256, 0, st>>>(b_col, fib_start, nfib, P, log2w, off);
     count_launch();
     PTC_CHECK_LAUNCH();
 }

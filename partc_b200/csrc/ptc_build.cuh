@@ -16,8 +16,8 @@ void launch_tuples(const uint32_t* idx, uint32_t order, const uint32_t* run_star
 void launch_fiber_len(const int32_t* a_fib, const uint32_t* fib_start, uint64_t n, uint64_t* len, cudaStream_t st);
 void launch_row_flops(const uint64_t* poff, const uint32_t* row_start, uint64_t nrows, uint64_t* flops,
                       cudaStream_t st);
-void launch_panel_offsets(const uint32_t* b_col, const uint32_t* b_fib, const uint32_t* fib_start, uint64_t nb,
-                          uint32_t P, uint32_t log2w, uint32_t* off, cudaStream_t st);
+void launch_panel_offsets(const uint32_t* b_col, const uint32_t* fib_start, uint64_t nfib, uint32_t P, uint32_t log2w,
+                          uint32_t* off, cudaStream_t st);
 
 // ---- canonical output order ----
 void launch_entry_keys(const uint32_t* row_of, const uint32_t* col_of, uint64_t n, uint32_t colbits, uint64_t* key,

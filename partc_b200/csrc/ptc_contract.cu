@@ -742,7 +742,7 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
     uint32_t* panel_off = nullptr;
     if (P > 1 && table_bytes(W) <= kPanelTableBytes) {
         panel_off = ar.alloc<uint32_t>(nfib * (uint64_t)(P + 1));
-        launch_panel_offsets(op.b_col, F.b_fib, op.fib_start, nb, P, pl.log2w, panel_off, st);
+        launch_panel_offsets(op.b_col, op.fib_start, nfib, P, pl.log2w, panel_off, st);
     }
     op.panel_off = panel_off;
     op.npanels = P;
