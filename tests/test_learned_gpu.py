@@ -1,5 +1,7 @@
 """The learned path: the sizer's predictions replace the symbolic pass; parts whose prediction was
 too small rerun exactly, so results stay identical to the reference's."""
+import os
+
 import numpy as np
 import pytest
 
@@ -67,3 +69,22 @@ def test_learned_path_without_sizer_is_an_error_or_uses_the_default(engine):
         engine.contract(t, None, c, modes, path="learned")
     except engine.PtcError as e:
         assert e.name == "PTC_ERR_INVALID_ARGUMENT"
+
+
+def test_trained_sizer_gains_over_an_untrained_one(engine, oracle_mod):
+    """What training buys: on a held-out Zipf contraction the shipped sizer (trained on the seeded
+    training contractions) predicts row sizes closely and needs no exact rerun, while the same
+    network with its initial weights is far off and reruns rows; both stay exact, and both skip
+    the exact symbolic pass of the large rows that the two-phase path runs."""
+    t = gen.random_coo([2482, 2862, 14036, 17], 400_000, [1.1] * 4, 2024, "uniform01")
+    o = oracle_mod.contract(t, None, 2, [0, 1, 2, 3])
+    trained = _lib.Sizer.load(os.path.join(os.path.dirname(_lib.LIB_PATH), "sizer_default.bin"))
+    untrained = _lib.Sizer.create(seed=5)
+    res = {}
+    for name, s in (("trained", trained), ("untrained", untrained)):
+        idx, vals, st = engine.contract(t, None, 2, [0, 1, 2, 3], path="learned", sizer=s.h.value)
+        assert_same_output(idx, vals, o["idx"], o["vals"], bit_exact=True)
+        res[name] = st
+    assert res["trained"]["sizer_mean_abs_log2_err"] < 0.25
+    assert res["trained"]["rerun_rows"] == 0
+    assert res["untrained"]["sizer_mean_abs_log2_err"] > 4 * res["trained"]["sizer_mean_abs_log2_err"]
