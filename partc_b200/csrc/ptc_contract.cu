@@ -1448,7 +1448,10 @@ void batch_impl(const std::vector<BatchItemHost>& items, uint32_t location, cons
         PTC_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev.device));
         PTC_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
         PTC_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used));
-        budget = (uint64_t)((free_b + (reserved > used ? reserved - used : 0)) * 0.6);
+        // leave room for sorting the work items by wave (item, key, index and gathered copy)
+        const uint64_t sort_need = (uint64_t)(pl.n_parts[0] + pl.n_parts[1]) * (2 * sizeof(PartItem) + 24);
+        const uint64_t avail = free_b + (reserved > used ? reserved - used : 0);
+        budget = avail > sort_need ? (uint64_t)((avail - sort_need) * 0.6) : (64ull << 20);
     }
     if (keep_device) budget = UINT64_MAX;  // every output stays: one wave
     std::vector<uint32_t> wave_item{0};
