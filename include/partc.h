@@ -188,8 +188,9 @@ typedef void (*ptc_batch_sink)(void* user, uint32_t item, const ptc_tensor* out)
 /*
  * Contract n independent items as one problem: every key of item i is offset into a key range of
  * its own, so one pass of each kernel (keys, sorts, one cuckoo table, symbolic pass) serves the
- * whole batch.  Outputs are produced in waves of consecutive items that fit opt->batch_wave_mib;
- * each wave's numeric pass is one CUDA-graph launch.  Results of every item equal ptc_contract's
+ * whole batch (items are taken in chunks of at most 32M nonzeros, so the working arrays stay a
+ * bounded share of the device).  Outputs are produced in waves of consecutive items that fit
+ * opt->batch_wave_mib; each wave's numeric pass is one CUDA-graph launch.  Results of every item equal ptc_contract's
  * (same entries; values bit-identical).
  *   outs != NULL: outs[i] receives item i's output (release each with ptc_tensor_free; items of a
  *                 wave share one block, freed with the last of them).  With PTC_DEVICE outputs

@@ -1861,6 +1861,63 @@ ptc_status ptc_self_contract(const uint32_t* hedges, const double* vals, uint32_
 namespace ptc {
 namespace {
 
+// A batch runs in chunks of consecutive items holding at most this many nonzeros (an item larger
+// than that is a chunk of its own): the build and planning arrays of a chunk, and its work items,
+// stay a bounded share of the device memory however long the batch is.
+constexpr uint64_t kBatchChunkNnz = 32ull << 20;
+
+void batch_chunks(const std::vector<BatchItemHost>& hi, uint32_t location, const ptc_options& opt,
+                  const BatchTarget& tg, ptc_stats& stats) {
+    size_t i0 = 0;
+    while (i0 < hi.size()) {
+        size_t i1 = i0;
+        uint64_t nnz = 0;
+        while (i1 < hi.size()) {
+            const uint64_t k = hi[i1].A->nnz + (hi[i1].self ? 0 : hi[i1].B->nnz);
+            if (i1 > i0 && nnz + k > kBatchChunkNnz) break;
+            nnz += k;
+            ++i1;
+        }
+        if (i0 == 0 && i1 == hi.size()) {
+            batch_impl(hi, location, opt, false, tg, stats);
+            return;
+        }
+        std::vector<BatchItemHost> part(hi.begin() + i0, hi.begin() + i1);
+        BatchTarget t2;
+        t2.outs = tg.outs;
+        t2.sink = tg.sink;
+        t2.user = tg.user;
+        t2.ids.assign(tg.ids.begin() + i0, tg.ids.begin() + i1);
+        ptc_stats s2;
+        std::memset(&s2, 0, sizeof(s2));
+        batch_impl(part, location, opt, false, t2, s2);
+        // sums over the chunks (times, counts); the largest of the per-chunk settings
+        stats.mult_adds += s2.mult_adds;
+        stats.out_nnz += s2.out_nnz;
+        stats.nrows += s2.nrows;
+        stats.ncols += s2.ncols;
+        stats.nfibers += s2.nfibers;
+        stats.a_nnz += s2.a_nnz;
+        stats.b_nnz += s2.b_nnz;
+        stats.t_total_ms += s2.t_total_ms;
+        stats.t_h2d_ms += s2.t_h2d_ms;
+        stats.t_build_ms += s2.t_build_ms;
+        stats.t_symbolic_ms += s2.t_symbolic_ms;
+        stats.t_numeric_ms += s2.t_numeric_ms;
+        stats.t_d2h_ms += s2.t_d2h_ms;
+        stats.hash_attempts = std::max(stats.hash_attempts, s2.hash_attempts);
+        stats.panel_width = std::max(stats.panel_width, s2.panel_width);
+        stats.rows_small += s2.rows_small;
+        stats.rows_hash += s2.rows_hash;
+        stats.hash_parts += s2.hash_parts;
+        stats.rows_long += s2.rows_long;
+        stats.rerun_rows += s2.rerun_rows;
+        stats.batch_waves += s2.batch_waves;
+        stats.rerun_items += s2.rerun_items;
+        i0 = i1;
+    }
+}
+
 // The items of a batch call, checked.
 std::vector<BatchItemHost> batch_host_items(const ptc_batch_item* items, uint32_t n, uint32_t& location) {
     PTC_REQUIRE(items != nullptr || n == 0, PTC_ERR_INVALID_ARGUMENT, "items is null");
@@ -1896,7 +1953,7 @@ double time_batch(const std::vector<BatchItemHost>& hi, uint32_t location, const
     for (uint32_t r = 0; r < repeats; ++r) {
         ptc_stats st;
         std::memset(&st, 0, sizeof(st));
-        batch_impl(hi, location, opt, false, tg, st);
+        batch_chunks(hi, location, opt, tg, st);
         t.push_back(st.t_total_ms);
     }
     std::sort(t.begin(), t.end());
@@ -1992,7 +2049,7 @@ ptc_status ptc_batch_contract(const ptc_batch_item* items, uint32_t n, const ptc
         }
         if (n > 0) {
             try {
-                batch_impl(hi, location, opt, false, tg, stats);
+                batch_chunks(hi, location, opt, tg, stats);
             } catch (...) {
                 if (outs)
                     for (uint32_t i = 0; i < n; ++i) ptc_tensor_free(&outs[i]);
