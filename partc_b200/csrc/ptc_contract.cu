@@ -211,7 +211,6 @@ struct Fibers {
     uint64_t n = 0;
     uint32_t* start = nullptr;  // [n + 1]
     uint64_t* key = nullptr;    // [n] contracted key of each fiber
-    uint32_t* of = nullptr;     // [nb] fiber of each sorted entry
     uint32_t* col = nullptr;    // [nb] column id of each sorted entry
     double* val = nullptr;      // [nb]
 };
@@ -238,10 +237,9 @@ Fibers group_fibers(const uint64_t* ckey, const uint32_t* col_rank, uint64_t nco
     uint64_t* ckey_sorted = ar.alloc<uint64_t>(nb);
     launch_gather<uint64_t>(ckey, fperm, nb, ckey_sorted, st);
     Fibers f;
-    f.of = ar.alloc<uint32_t>(nb);
     f.start = ar.alloc<uint32_t>(nb + 1);
     f.key = ar.alloc<uint64_t>(std::max<uint64_t>(nb, 1));
-    f.n = runs_of_sorted(ckey_sorted, nb, f.of, f.start, f.key, ar);
+    f.n = runs_of_sorted(ckey_sorted, nb, nullptr, f.start, f.key, ar);
     f.col = ar.alloc<uint32_t>(nb);
     f.val = ar.alloc<double>(nb);
     launch_gather<uint32_t>(col_id ? col_id : col_rank, fperm, nb, f.col, st);
@@ -562,14 +560,12 @@ struct Collect {
 // item's rows and columns lie.
 struct Front {
     Operands op;
-    const uint32_t* b_fib = nullptr;  // fiber of each sorted B entry
     const uint32_t* a_row = nullptr;  // row of each sorted A element
     bool batch = false;
     uint32_t nitems = 1;
     uint32_t* row_first = nullptr;        // device [nitems + 1]: item i owns rows [row_first[i], row_first[i+1])
     std::vector<uint32_t> h_row_first;    // host copy
-    std::vector<uint32_t> colbase;        // first global column of each item
-    std::vector<uint32_t> item_fa, item_fb;
+    std::vector<uint32_t> colbase;        // first global column of each item (nitems + 1 entries)
     ItemOut* item_out = nullptr;          // device [nitems], filled per wave
 };
 
@@ -949,14 +945,11 @@ Front front_single(const ptc_coo* A, const ptc_coo* B, bool self, uint32_t c, co
     op.b_col = fib.col; op.b_val = fib.val; op.fib_start = fib.start;
     op.row_tuple = row_tuple; op.col_tuple = col_tuple;
     op.err = err;
-    F.b_fib = fib.of;
     F.a_row = rows.run_of;
     F.h_row_first = {0u, (uint32_t)rows.nruns};
     F.row_first = ar.alloc<uint32_t>(2);
     PTC_CUDA(cudaMemcpyAsync(F.row_first, F.h_row_first.data(), 2 * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-    F.colbase = {0u};
-    F.item_fa = {fa};
-    F.item_fb = {fb};
+    F.colbase = {0u, (uint32_t)ncols};
     stats.ncols = ncols;
     return F;
 }
@@ -1351,18 +1344,11 @@ Front front_batch(const std::vector<BatchItemHost>& items, uint32_t location, co
     op.row_item = row_item;
     F.item_out = ar.alloc<ItemOut>(n);
     op.item_out = F.item_out;
-    F.b_fib = fib.of;
     F.a_row = rows.run_of;
     F.batch = true;
     F.nitems = n;
     F.row_first = row_first;
     F.colbase = h_col_first;
-    F.item_fa.resize(n);
-    F.item_fb.resize(n);
-    for (uint32_t i = 0; i < n; ++i) {
-        F.item_fa[i] = items[i].fa;
-        F.item_fb[i] = items[i].fb;
-    }
     stats.ncols = cols.nruns;
     return F;
 }
