@@ -727,7 +727,9 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
     if (W == 0) {  // at most 256 columns (a third of a dense warp task), wider for small tables
         W = 32;
         while (W < 256 && (uint64_t)W * 16 < ncols) W <<= 1;
-        while (W < warp_task_dense_columns() && panel_entries(W) * 4 > (2ull << 30)) W <<= 1;
+        // wider panels for big tables, but never wider than a dense warp task (a single panel
+        // above a sparse task's capacity becomes a dense task over that panel)
+        while (2 * W <= warp_task_dense_columns() && panel_entries(W) * 4 > (2ull << 30)) W <<= 1;
     }
     PTC_REQUIRE(W <= hash_part_capacity(), PTC_ERR_INVALID_ARGUMENT, "panel_width larger than a hash part");
     pl.W = W;
