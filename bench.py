@@ -302,7 +302,8 @@ def run_batch(args, rank, world, local):
         return items
 
     items = make_items(di.data_ptr(), dv.data_ptr(), _lib.PTC_DEVICE)
-    opts = dict(device=local, stream=stream.cuda_stream, path=args.path)
+    path = args.batch_path
+    opts = dict(device=local, stream=stream.cuda_stream, path=path)
     sizes = {}
 
     def sink(i, t):
@@ -328,6 +329,22 @@ def run_batch(args, rank, world, local):
     ms = pdist.max_over_ranks(ev0.elapsed_time(ev1), device=dev)
     value = pdist.job_throughput(M, args.steps, world, ms * 1e-3)
     na = int(sum(w.tensor.nnz for w in work))
+    # the other path on the same batch, timed the same way
+    paths = {path: {"value": value, "ms_per_step": ms / args.steps, "rerun_items": int(stats[0]["rerun_items"])}}
+    if args.compare_paths:
+        other = "learned" if path == "two_phase" else "two_phase"
+        oo = dict(opts, path=other)
+        _lib.batch_contract(items, outputs="none", **oo)
+        torch.cuda.synchronize()
+        ost = []
+        ev0.record(stream)
+        for _ in range(args.steps):
+            ost.append(_lib.batch_contract(items, outputs="none", **oo)[1])
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        oms = pdist.max_over_ranks(ev0.elapsed_time(ev1), device=dev)
+        paths[other] = {"value": pdist.job_throughput(M, args.steps, world, oms * 1e-3),
+                        "ms_per_step": oms / args.steps, "rerun_items": int(ost[0]["rerun_items"])}
     alg = 12 * na + 12 * M + out_bytes
     t_num = statistics.mean(s["t_numeric_ms"] for s in stats) * 1e-3
     peak, peak_kind = measured_hbm_peak()
@@ -367,7 +384,7 @@ def run_batch(args, rank, world, local):
         pdist.barrier()
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
-            _lib.batch_contract(hitems, outputs="none", device=local, stream=stream.cuda_stream, path=args.path)
+            _lib.batch_contract(hitems, outputs="none", device=local, stream=stream.cuda_stream, path=path)
         el = pdist.max_over_ranks(time.perf_counter() - t0, device=dev)
         e2e = {"value": pdist.job_throughput(M, args.e2e_steps, world, el), "unit": "mult-adds/s",
                "h2d_bytes_per_step": int(idx_cat.nbytes + val_cat.nbytes), "d2h_bytes_per_step": 8 * n,
@@ -379,14 +396,14 @@ def run_batch(args, rank, world, local):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded generator partc_b200/gen.py batch_member, seeds 0..n-1)",
-            "config": {"workload": f"batch{n}", "items": n, "nnz": na, "path": args.path,
+            "config": {"workload": f"batch{n}", "items": n, "nnz": na, "path": path,
                        "parallelism": f"replicas x{world}", "mult_adds_per_step": M, "out_nnz_per_step": R,
                        "l2": "no flush needed: each step writes its outputs (>> 126 MB L2)"},
             "phase_ms": {k: statistics.mean(s[k] for s in stats) for k in
                          ("t_build_ms", "t_symbolic_ms", "t_numeric_ms", "t_d2h_ms", "t_total_ms")},
             "batch_waves": stats[0]["batch_waves"], "rerun_items": stats[0]["rerun_items"],
             "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
-            "roofline": roofline, "per_contraction": loop, "e2e": e2e, "cpu_baseline": None,
+            "roofline": roofline, "per_contraction": loop, "paths": paths, "e2e": e2e, "cpu_baseline": None,
             "clocks": clk.summary(),
         }
         print(json.dumps(line))
@@ -406,6 +423,7 @@ def main():
     ap.add_argument("--cpu-target-flops", type=float, default=6e7)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-items", type=int, default=4096)
+    ap.add_argument("--batch-path", default="two_phase", choices=["two_phase", "learned"])
     ap.add_argument("--no-cusparse", dest="cusparse", action="store_false")
     ap.add_argument("--no-per-contraction", dest="per_contraction", action="store_false")
     args = ap.parse_args()
