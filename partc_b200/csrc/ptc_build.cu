@@ -184,6 +184,19 @@ void launch_panel_offsets(const uint32_t* b_col, const uint32_t* fib_start, uint
 
 namespace ptc {
 
+// key[i] = rows[i] (as a 64-bit sort key)
+__global__ void row_keys_kernel(const uint32_t* __restrict__ rows, uint64_t n, uint64_t* __restrict__ key) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) key[i] = rows[i];
+}
+
+void launch_row_keys(const uint32_t* rows, uint64_t n, uint64_t* key, cudaStream_t st) {
+    if (n == 0) return;
+    row_keys_kernel<<<ceil_div_u32(n, 256), 256, 0, st>>>(rows, n, key);
+    count_launch();
+    PTC_CHECK_LAUNCH();
+}
+
 // canonical output order: key[e] = row_of[e] << colbits | col_of[e], perm[e] = e
 __global__ void entry_keys_kernel(const uint32_t* __restrict__ row_of, const uint32_t* __restrict__ col_of, uint64_t n,
                                   uint32_t colbits, uint64_t* __restrict__ key, uint32_t* __restrict__ perm) {

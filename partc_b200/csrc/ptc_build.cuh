@@ -19,6 +19,9 @@ void launch_row_flops(const uint64_t* poff, const uint32_t* row_start, uint64_t 
 void launch_panel_offsets(const uint32_t* b_col, const uint32_t* fib_start, uint64_t nfib, uint32_t P, uint32_t log2w,
                           uint32_t* off, cudaStream_t st);
 
+// key[i] = rows[i]
+void launch_row_keys(const uint32_t* rows, uint64_t n, uint64_t* key, cudaStream_t st);
+
 // ---- canonical output order ----
 void launch_entry_keys(const uint32_t* row_of, const uint32_t* col_of, uint64_t n, uint32_t colbits, uint64_t* key,
                        uint32_t* perm, cudaStream_t st);

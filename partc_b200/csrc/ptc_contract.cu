@@ -616,6 +616,11 @@ struct Plan {
     PartItem* parts[2] = {nullptr, nullptr};
     uint32_t n_parts[2] = {0, 0};
     uint32_t* work_counter = nullptr;
+    // collision-free large rows (two-phase path): written product by product, in row order
+    uint64_t* alen = nullptr;        // exclusive scan of the A nonzeros' fiber lengths
+    uint32_t* copy_rows = nullptr;
+    uint64_t* copy_keys = nullptr;   // the same row ids as sort keys (wave slices)
+    uint32_t n_copy = 0;
     bool collected = false;
 };
 
@@ -641,6 +646,7 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
     exclusive_scan<uint64_t>(alen, alen, na, ar);
     pl.row_flops = ar.alloc<uint64_t>(std::max<uint64_t>(nrows, 1));
     launch_row_flops(alen, op.row_start, nrows, pl.row_flops, st);
+    pl.alen = alen;
     pl.flops = read_scalar(alen + na, st);
     stats.mult_adds = pl.flops;
     stats.nrows = nrows;
@@ -855,19 +861,39 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
         pl.claim_total = read_scalar(pl.claim_off + nrows, st);
     }
 
+    // exact sizes: the collision-free large rows need no table (launch_copy_rows)
+    const uint64_t* skip_off = pl.learned ? nullptr : pl.row_off;
+    const uint64_t* skip_flops = pl.learned ? nullptr : pl.row_flops;
+    if (!pl.learned && n_big > 0) {
+        uint32_t* flag = ar.alloc<uint32_t>((uint64_t)n_big + 1);
+        uint32_t* pos = ar.alloc<uint32_t>((uint64_t)n_big + 1);
+        launch_copy_flags(pl.big_rows, n_big, pl.row_off, pl.row_flops, flag, st);
+        exclusive_scan<uint32_t>(flag, pos, n_big, ar);
+        pl.n_copy = read_scalar(pos + n_big, st);
+        if (pl.n_copy > 0) {
+            uint32_t* sel = ar.alloc<uint32_t>(pl.n_copy);
+            launch_compact_indices(flag, pos, n_big, sel, st);  // positions in big_rows
+            pl.copy_rows = ar.alloc<uint32_t>(pl.n_copy);
+            launch_gather<uint32_t>(pl.big_rows, sel, pl.n_copy, pl.copy_rows, st);
+            pl.copy_keys = ar.alloc<uint64_t>(pl.n_copy);
+            launch_row_keys(pl.copy_rows, pl.n_copy, pl.copy_keys, st);
+            radix_sort_pairs(pl.copy_keys, pl.copy_rows, pl.n_copy, 0, bits_for_space(nrows), ar);
+        }
+    }
+
     // split large rows into tasks / parts that fit a shared-memory table
     for (int kind = 0; kind < 2; ++kind) {
         const uint64_t r0 = kind == 0 ? 0 : pl.n_warp_rows, nr = kind == 0 ? pl.n_warp_rows : n_big - pl.n_warp_rows;
         uint32_t* nparts = ar.alloc<uint32_t>(nr + 1);
         const uint32_t* pc = pbase ? panel_cnt : panel_cnt + r0 * P;
         const uint64_t* pb = pbase ? pbase + r0 : nullptr;
-        launch_count_parts(pc, pb, nr, P, pl.rule[kind], nparts, op.err, st);
+        launch_count_parts(pl.big_rows + r0, pc, pb, nr, P, pl.rule[kind], skip_off, skip_flops, nparts, op.err, st);
         exclusive_scan<uint32_t>(nparts, nparts, nr, ar);
         pl.n_parts[kind] = read_scalar(nparts + nr, st);
         PTC_REQUIRE(read_scalar(op.err, st) == 0, PTC_ERR_INTERNAL, "a fine panel exceeds the hash part capacity");
         pl.parts[kind] = ar.alloc<PartItem>(pl.n_parts[kind]);
         launch_fill_parts(pl.big_rows + r0, pc, pb, nr, P, pl.rule[kind], nparts, pl.learned ? nullptr : pl.row_off,
-                          pl.parts[kind], st);
+                          skip_flops, pl.parts[kind], st);
     }
     stats.hash_parts = pl.n_parts[0] + pl.n_parts[1];
     return pl;
@@ -1023,6 +1049,7 @@ void contract_impl(const ptc_coo* A, const ptc_coo* Bin, uint32_t c, const uint3
         }
         std::vector<Launched> groups;
         launch_small_rows(true, op, pl.small_rows, pl.n_small, nullptr, pl.row_off, ov, st);
+        launch_copy_rows(op, pl.copy_rows, pl.n_copy, pl.alen, pl.row_off, ov, dev.num_sms, st);
         for (int kind = 0; kind < 2; ++kind) {
             OutputView o = ov;
             if (learned) {
@@ -1486,6 +1513,16 @@ void batch_impl(const std::vector<BatchItemHost>& items, uint32_t location, cons
         PTC_CUDA(cudaStreamSynchronize(st));
     }
     const std::vector<uint32_t> sb = read_at<uint32_t>(pl.small_pos, wave_row, ar);
+    std::vector<uint32_t> cb(nw + 1, 0);  // collision-free rows of each wave (sorted by row)
+    if (pl.n_copy > 0) {
+        std::vector<uint64_t> wr64(wave_row.begin(), wave_row.end());
+        uint64_t* wr_d = ar.alloc<uint64_t>(nw + 1);
+        PTC_CUDA(cudaMemcpyAsync(wr_d, wr64.data(), (nw + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+        uint32_t* cbd = ar.alloc<uint32_t>(nw + 2);
+        launch_key_bounds(pl.copy_keys, pl.n_copy, wr_d, nw + 1, cbd, st);
+        PTC_CUDA(cudaMemcpyAsync(cb.data(), cbd, (nw + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        PTC_CUDA(cudaStreamSynchronize(st));
+    }
     std::vector<uint32_t> rb(nw + 1, 0);
     if (pl.n_esc > 0) rb = read_at<uint32_t>(pl.esc_first, read_at<uint32_t>(pl.esc_pos, wave_row, ar), ar);
 
@@ -1583,7 +1620,7 @@ void batch_impl(const std::vector<BatchItemHost>& items, uint32_t location, cons
                 }
             PTC_CUDA(cudaEventRecord(ev.ev[EV_WAVE0], st));
             const bool work = sb[w + 1] > sb[w] || pb[0][w + 1] > pb[0][w] || pb[1][w + 1] > pb[1][w] ||
-                              rb[w + 1] > rb[w];
+                              rb[w + 1] > rb[w] || cb[w + 1] > cb[w];
             // the wave's numeric pass, captured and launched as one graph
             cudaGraph_t graph = nullptr;
             cudaGraphExec_t exec = nullptr;
@@ -1592,6 +1629,8 @@ void batch_impl(const std::vector<BatchItemHost>& items, uint32_t location, cons
                 try {
                     launch_small_rows(true, op, pl.small_rows + sb[w], sb[w + 1] - sb[w], nullptr, pl.row_off, ov,
                                       st);
+                    launch_copy_rows(op, pl.copy_rows + cb[w], cb[w + 1] - cb[w], pl.alen, pl.row_off, ov,
+                                     dev.num_sms, st);
                     for (int kind = 0; kind < 2; ++kind)
                         launch_parts(kind, op, parts[kind] + pb[kind][w], pb[kind][w + 1] - pb[kind][w], ovk[kind],
                                      pl.work_counter, op.err, dev.num_sms, st);

@@ -134,11 +134,21 @@ __device__ __forceinline__ void row_panels(const uint64_t* pbase, uint64_t i, ui
     n = pbase ? (uint32_t)(pbase[i + 1] - pbase[i]) : P;
 }
 
-__global__ void count_parts_kernel(const uint32_t* __restrict__ panel_cnt, const uint64_t* __restrict__ pbase,
-                                   uint64_t nbig, uint32_t P, SplitRule rule, uint32_t* __restrict__ nparts,
-                                   uint32_t* __restrict__ oversize) {
+// a large row whose exact output count equals its products: no two products share a column
+__device__ __forceinline__ bool collision_free(const uint64_t* row_off, const uint64_t* row_flops, uint32_t row) {
+    return row_off && row_flops && row_off[row + 1] - row_off[row] == row_flops[row];
+}
+
+__global__ void count_parts_kernel(const uint32_t* __restrict__ rows, const uint32_t* __restrict__ panel_cnt,
+                                   const uint64_t* __restrict__ pbase, uint64_t nbig, uint32_t P, SplitRule rule,
+                                   const uint64_t* __restrict__ row_off, const uint64_t* __restrict__ row_flops,
+                                   uint32_t* __restrict__ nparts, uint32_t* __restrict__ oversize) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nbig) return;
+    if (collision_free(row_off, row_flops, rows[i])) {
+        nparts[i] = 0;
+        return;
+    }
     uint64_t b;
     uint32_t n;
     row_panels(pbase, i, P, b, n);
@@ -147,11 +157,26 @@ __global__ void count_parts_kernel(const uint32_t* __restrict__ panel_cnt, const
     if (over) atomicOr(oversize, 1u);
 }
 
-void launch_count_parts(const uint32_t* panel_cnt, const uint64_t* pbase, uint64_t nbig, uint32_t npanels,
-                        SplitRule rule, uint32_t* nparts, uint32_t* oversize, cudaStream_t st) {
+void launch_count_parts(const uint32_t* rows, const uint32_t* panel_cnt, const uint64_t* pbase, uint64_t nbig,
+                        uint32_t npanels, SplitRule rule, const uint64_t* row_off, const uint64_t* row_flops,
+                        uint32_t* nparts, uint32_t* oversize, cudaStream_t st) {
     if (nbig == 0) return;
-    count_parts_kernel<<<ceil_div_u32(nbig, 256), 256, 0, st>>>(panel_cnt, pbase, nbig, npanels, rule, nparts,
-                                                                oversize);
+    count_parts_kernel<<<ceil_div_u32(nbig, 256), 256, 0, st>>>(rows, panel_cnt, pbase, nbig, npanels, rule, row_off,
+                                                                row_flops, nparts, oversize);
+    count_launch();
+    PTC_CHECK_LAUNCH();
+}
+
+__global__ void copy_flags_kernel(const uint32_t* __restrict__ rows, uint64_t n, const uint64_t* __restrict__ row_off,
+                                  const uint64_t* __restrict__ row_flops, uint32_t* __restrict__ flag) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) flag[i] = collision_free(row_off, row_flops, rows[i]) ? 1u : 0u;
+}
+
+void launch_copy_flags(const uint32_t* rows, uint64_t n, const uint64_t* row_off, const uint64_t* row_flops,
+                       uint32_t* flag, cudaStream_t st) {
+    if (n == 0) return;
+    copy_flags_kernel<<<ceil_div_u32(n, 256), 256, 0, st>>>(rows, n, row_off, row_flops, flag);
     count_launch();
     PTC_CHECK_LAUNCH();
 }
@@ -159,10 +184,11 @@ void launch_count_parts(const uint32_t* panel_cnt, const uint64_t* pbase, uint64
 __global__ void fill_parts_kernel(const uint32_t* __restrict__ rows, const uint32_t* __restrict__ panel_cnt,
                                   const uint64_t* __restrict__ pbase, uint64_t nbig, uint32_t P, SplitRule rule,
                                   const uint32_t* __restrict__ part_pos, const uint64_t* __restrict__ row_off,
-                                  PartItem* __restrict__ parts) {
+                                  const uint64_t* __restrict__ row_flops, PartItem* __restrict__ parts) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nbig) return;
     const uint32_t row = rows[i];
+    if (collision_free(row_off, row_flops, row)) return;
     const uint64_t base = row_off ? row_off[row] : 0;  // no offsets: the parts claim output later
     uint64_t b;
     uint32_t n;
@@ -182,10 +208,10 @@ __global__ void fill_parts_kernel(const uint32_t* __restrict__ rows, const uint3
 
 void launch_fill_parts(const uint32_t* rows, const uint32_t* panel_cnt, const uint64_t* pbase, uint64_t nbig,
                        uint32_t npanels, SplitRule rule, const uint32_t* part_pos, const uint64_t* row_off,
-                       PartItem* parts, cudaStream_t st) {
+                       const uint64_t* row_flops, PartItem* parts, cudaStream_t st) {
     if (nbig == 0) return;
     fill_parts_kernel<<<ceil_div_u32(nbig, 256), 256, 0, st>>>(rows, panel_cnt, pbase, nbig, npanels, rule, part_pos,
-                                                               row_off, parts);
+                                                               row_off, row_flops, parts);
     count_launch();
     PTC_CHECK_LAUNCH();
 }

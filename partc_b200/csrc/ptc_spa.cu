@@ -580,6 +580,44 @@ void launch_warp_tasks(const Operands& op, const PartItem* tasks, uint32_t ntask
 }
 
 // ---------------------------------------------------------------------------------------------
+// numeric pass, collision-free rows: a large row whose exact output count equals its products has
+// no two products in one column, so each product is an output entry of its own (a single term:
+// no sum, no table).  Block per row, warps over its A nonzeros, lanes over each fiber: entry
+// (k, j) goes to row_off[row] + (products before k in the row) + (j - fiber start).
+// ---------------------------------------------------------------------------------------------
+
+constexpr int kCopyThreads = 256;
+
+__global__ void __launch_bounds__(kCopyThreads)
+    copy_rows_kernel(Operands op, const uint32_t* __restrict__ rows, uint32_t nrows,
+                     const uint64_t* __restrict__ alen, const uint64_t* __restrict__ row_off, OutputView out) {
+    const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+    for (uint32_t i = blockIdx.x; i < nrows; i += gridDim.x) {
+        const uint32_t row = rows[i];
+        const uint32_t ka = op.row_start[row], kb = op.row_start[row + 1];
+        const uint64_t base = row_off[row] - alen[ka];
+        for (uint32_t k = ka + warp; k < kb; k += kCopyThreads / 32) {
+            const int32_t f = op.a_fib[k];
+            if (f < 0) continue;
+            const uint32_t s = op.fib_start[f], e = op.fib_start[f + 1];
+            const double a = op.a_val[k];
+            const uint64_t o = base + alen[k];
+            for (uint32_t j = s + lane; j < e; j += 32)
+                write_entry(op, out, o + (j - s), row, __ldg(op.b_col + j), __dmul_rn(a, __ldg(op.b_val + j)));
+        }
+    }
+}
+
+void launch_copy_rows(const Operands& op, const uint32_t* rows, uint32_t nrows, const uint64_t* alen,
+                      const uint64_t* row_off, const OutputView& out, int num_sms, cudaStream_t st) {
+    if (nrows == 0) return;
+    const uint32_t grid = std::min<uint32_t>(nrows, (uint32_t)num_sms * 8);
+    copy_rows_kernel<<<grid, kCopyThreads, 0, st>>>(op, rows, nrows, alen, row_off, out);
+    count_launch();
+    PTC_CHECK_LAUNCH();
+}
+
+// ---------------------------------------------------------------------------------------------
 // numeric pass for the other rows: one block per part (a row's columns in fine panels [p0, p1)).
 // A dense part indexes its accumulator by column directly; a sparse part uses an open-addressing
 // table.  Both live in the same shared-memory region.

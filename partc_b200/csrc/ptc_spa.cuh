@@ -38,6 +38,11 @@ constexpr uint32_t kWarpTaskMaxLen = 1024;
 void launch_warp_tasks(const Operands& op, const PartItem* tasks, uint32_t ntasks, const OutputView& out,
                        uint32_t* work_counter, uint32_t* overflow, int num_sms, cudaStream_t st);
 
+// collision-free large rows (exact output count = products), numeric: each product an entry;
+// alen = exclusive scan of the A nonzeros' fiber lengths, row_off the rows' exact offsets
+void launch_copy_rows(const Operands& op, const uint32_t* rows, uint32_t nrows, const uint64_t* alen,
+                      const uint64_t* row_off, const OutputView& out, int num_sms, cudaStream_t st);
+
 // other rows, numeric: one block per part
 void launch_hash_parts(const Operands& op, const PartItem* parts, uint32_t nparts, const OutputView& out,
                        uint32_t* work_counter, uint32_t* overflow, int num_sms, cudaStream_t st);
@@ -87,11 +92,17 @@ struct SplitRule {
 };
 // number of parts of each big row; sets *oversize if one fine panel alone exceeds cap.  Row i's
 // panel counts are panel_cnt[pbase[i] .. pbase[i+1]), or panel_cnt[i * npanels ..] with pbase null.
-void launch_count_parts(const uint32_t* panel_cnt, const uint64_t* pbase, uint64_t nbig, uint32_t npanels,
-                        SplitRule rule, uint32_t* nparts, uint32_t* oversize, cudaStream_t st);
+// With row_off and row_flops given (exact sizes), rows whose output count equals their products
+// get no parts (the collision-free rows, written by launch_copy_rows).
+void launch_count_parts(const uint32_t* rows, const uint32_t* panel_cnt, const uint64_t* pbase, uint64_t nbig,
+                        uint32_t npanels, SplitRule rule, const uint64_t* row_off, const uint64_t* row_flops,
+                        uint32_t* nparts, uint32_t* oversize, cudaStream_t st);
+// flag[i] = 1 if rows[i]'s exact output count equals its products
+void launch_copy_flags(const uint32_t* rows, uint64_t n, const uint64_t* row_off, const uint64_t* row_flops,
+                       uint32_t* flag, cudaStream_t st);
 void launch_fill_parts(const uint32_t* rows, const uint32_t* panel_cnt, const uint64_t* pbase, uint64_t nbig,
                        uint32_t npanels, SplitRule rule, const uint32_t* part_pos, const uint64_t* row_off,
-                       PartItem* parts, cudaStream_t st);
+                       const uint64_t* row_flops, PartItem* parts, cudaStream_t st);
 // np[i] = panels of rows[i]'s item (a batch): ceil(item_cols[row_item[row]] / 2^log2w), at least 1
 void launch_row_panel_counts(const uint32_t* rows, uint64_t n, const uint32_t* row_item, const uint32_t* item_cols,
                              uint32_t log2w, uint64_t* np, cudaStream_t st);
