@@ -81,3 +81,28 @@ def test_self_contraction_of_one_nonzero_is_an_error(L):
     with pytest.raises(_lib.PtcError) as e:
         L.contract(t, None, 2, [0, 1, 2])
     assert e.value.name == "PTC_ERR_TOO_FEW_NONZEROS"
+
+
+def test_binding_layouts_match_the_header(L, tmp_path):
+    """Every struct the ctypes binding mirrors has the header's size and field offsets (compiled
+    with the host C compiler against include/partc.h)."""
+    import subprocess
+    structs = {"ptc_coo": _lib.Coo, "ptc_tensor": _lib.Tensor, "ptc_options": _lib.Options,
+               "ptc_stats": _lib.Stats, "ptc_batch_item": _lib.BatchItem, "ptc_tune_report": _lib.TuneReport,
+               "ptc_train_options": _lib.TrainOptions, "ptc_train_stats": _lib.TrainStats}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "partc.h"', "int main(void) {"]
+    for cname, cls in structs.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in cls._fields_:
+            lines.append(f'printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for cname, cls in structs.items():
+        assert got[(cname, "size")] == C.sizeof(cls), cname
+        for fname, _ in cls._fields_:
+            assert got[(cname, fname)] == getattr(cls, fname).offset, (cname, fname)
