@@ -291,7 +291,11 @@ extern "C" ptc_status ptc_read_tns(const char* path, const ptc_options* opt_in, 
             out->location = PTC_HOST;
             out->idx = static_cast<uint32_t*>(std::malloc(std::max<uint64_t>((uint64_t)nnz * d, 1) * 4));
             out->vals = static_cast<double*>(std::malloc(std::max<uint64_t>(nnz, 1) * 8));
-            PTC_REQUIRE(out->idx && out->vals, PTC_ERR_OUT_OF_MEMORY, "host allocation failed");
+            if (!out->idx || !out->vals) {
+                cudaFreeAsync(oidx, st);
+                cudaFreeAsync(oval, st);
+                throw Error{PTC_ERR_OUT_OF_MEMORY, "host allocation failed"};
+            }
             PTC_CUDA(cudaMemcpyAsync(out->idx, oidx, (uint64_t)nnz * d * 4, cudaMemcpyDeviceToHost, st));
             PTC_CUDA(cudaMemcpyAsync(out->vals, oval, (uint64_t)nnz * 8, cudaMemcpyDeviceToHost, st));
             PTC_CUDA(cudaFreeAsync(oidx, st));
