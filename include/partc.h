@@ -86,8 +86,9 @@ typedef struct ptc_options {
     uint32_t output_location;  /* PTC_HOST (default, like the reference) or PTC_DEVICE */
     uint32_t verbose;          /* 1: print the reference's stdout lines (timings, nnz) */
     uint32_t panel_width;      /* columns per fine panel (power of two in [32, 4096]); large
-                                  rows are cut at panel boundaries into parts and each warp owns
-                                  a range of panels; 0 = automatic */
+                                  rows are cut at panel boundaries into work items (a warp's or a
+                                  block's range of panels); above 512 only block parts are used;
+                                  0 = automatic (at most 256 unless the counters grow too big) */
     uint64_t hash_seed;        /* seed of the cuckoo hash family */
     const ptc_sizer* sizer;    /* PTC_PATH_LEARNED: trained sizer (NULL = built-in weights) */
     uint32_t sort_rows;        /* 1: rows of the output in increasing free-key order and every
