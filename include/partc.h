@@ -41,7 +41,7 @@ typedef enum ptc_status {
                                      fksCuckoo.hpp:244-247) */
     PTC_ERR_CUDA = 8,             /* a CUDA runtime call failed */
     PTC_ERR_NO_DEVICE = 9,        /* no usable sm_100 device */
-    PTC_ERR_DEVICE_TIMEOUT = 10,  /* a bounded device-side wait gave up */
+                                  /* 10 is not used (no device-side wait exists to time out) */
     PTC_ERR_OVERFLOW = 11,        /* a result does not fit the caller-provided capacity */
     PTC_ERR_INTERNAL = 12
 } ptc_status;
@@ -105,6 +105,14 @@ typedef struct ptc_options {
                                        MiB (default: 60% of the free memory) */
     uint32_t warp_task_max_len;     /* large rows with at most this many A nonzeros use one warp per
                                        column range, longer ones one block per part (default 1024) */
+    /* cuckoo build of B's fiber table (the reference's buildHashTable, fksCuckoo.hpp:1044-1060) */
+    uint32_t cuckoo_max_chain;      /* evictions one insertion may cause before the build attempt
+                                       fails (default 64; 0 = no eviction at all) -- set it small to
+                                       exercise the rebuild path */
+    uint32_t cuckoo_max_attempts;   /* builds tried, each with new hash seeds and, after every two
+                                       failures, twice the buckets (the reference's rehash with new
+                                       kDict pairs and a larger table, fksCuckoo.hpp:297-442), before
+                                       the call returns PTC_ERR_HASH_BUILD (default 8) */
     uint32_t reserved[2];
 } ptc_options;
 
@@ -244,6 +252,12 @@ ptc_status ptc_autotune(const ptc_batch_item* items, uint32_t n, const ptc_optio
 /* Number of CUDA devices the library can use (sm_100 class). */
 int ptc_device_count(void);
 
+/* Bytes of the device's stream-ordered memory pool (the pool every call allocates its working
+ * arrays and device outputs from) that are allocated and not yet freed, after the device has
+ * finished the work queued so far.  Device outputs a caller still holds count; with none held,
+ * a finished call -- successful or failed -- leaves 0 behind. */
+ptc_status ptc_device_pool_in_use(int32_t device, uint64_t* bytes);
+
 /* ---- learned sizer (no counterpart in the reference: it replaces the symbolic pass) ----
  * A 16 -> 64 -> 64 -> 1 ReLU network with BF16 weights and FP32 accumulation that predicts
  * log2(1 + output nnz) of a row from per-row features computed on the device.  It is trained
@@ -295,10 +309,12 @@ ptc_status ptc_sizer_predict(const ptc_sizer* s, const float* features, uint64_t
  * owns the device, or an allocation would synchronize the device or is not allowed there).  Its
  * device scratch -- the BF16 weights, up to 65536 staged feature rows and their predictions -- is
  * one static device array of about 4.3 MiB that every device loading the library keeps until the
- * process exits.  n > 65536 is rejected with PTC_ERR_INVALID_ARGUMENT.  The first call on a device
- * looks up that array's address; make it before capturing any stream.  All calls share the array:
- * calls whose GPU work overlaps race on it.  Runs on the calling thread's per-thread default
- * stream and returns when out holds the predictions (host arrays in and out). */
+ * process exits.  n > 65536 is rejected with PTC_ERR_INVALID_ARGUMENT.  Every call looks up that
+ * array's address on the device (an allocation-free lookup); the first call on a device also loads
+ * the library's device code there, so make it before capturing any stream.  All calls share the
+ * array: calls whose GPU work overlaps race on it.  Runs on the calling thread's per-thread
+ * default stream, restores the caller's current device and returns when out holds the
+ * predictions (host arrays in and out). */
 ptc_status ptc_sizer_predict_noalloc(const ptc_sizer* s, const float* features, uint64_t n,
                                      int32_t device, float* out);
 /* Gradient of the mean squared error over n samples (host arrays; grads has PTC_SIZER_PARAMS). */

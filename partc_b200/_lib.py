@@ -21,7 +21,7 @@ PATH_TWO_PHASE, PATH_LEARNED = 0, 1
 STATUS = {
     0: "PTC_OK", 1: "PTC_ERR_INVALID_ARGUMENT", 2: "PTC_ERR_INDEX_RANGE", 3: "PTC_ERR_KEY_OVERFLOW",
     4: "PTC_ERR_EMPTY_CONTRACTION", 5: "PTC_ERR_TOO_FEW_NONZEROS", 6: "PTC_ERR_HASH_BUILD",
-    7: "PTC_ERR_OUT_OF_MEMORY", 8: "PTC_ERR_CUDA", 9: "PTC_ERR_NO_DEVICE", 10: "PTC_ERR_DEVICE_TIMEOUT",
+    7: "PTC_ERR_OUT_OF_MEMORY", 8: "PTC_ERR_CUDA", 9: "PTC_ERR_NO_DEVICE",
     11: "PTC_ERR_OVERFLOW", 12: "PTC_ERR_INTERNAL",
 }
 
@@ -32,6 +32,7 @@ EXPORTS = [
     "ptc_sizer_save", "ptc_sizer_free", "ptc_sizer_get_params", "ptc_sizer_set_params", "ptc_sizer_collect",
     "ptc_sizer_train", "ptc_sizer_predict", "ptc_sizer_gradients", "ptc_buffer_free",
     "ptc_sizer_predict_noalloc", "ptc_batch_contract", "ptc_autotune", "ptc_read_tns", "ptc_write_tns",
+    "ptc_device_pool_in_use",
 ]
 SIZER_FEATURES = 16
 SIZER_PARAMS = 5313
@@ -60,7 +61,8 @@ class Options(C.Structure):
                 ("panel_width", C.c_uint32), ("hash_seed", C.c_uint64), ("sizer", C.c_void_p),
                 ("sort_rows", C.c_uint32), ("small_max_products", C.c_uint32),
                 ("sort_max_avg_products", C.c_uint32), ("hash_load_pct", C.c_uint32),
-                ("batch_wave_mib", C.c_uint32), ("warp_task_max_len", C.c_uint32), ("reserved", C.c_uint32 * 2)]
+                ("batch_wave_mib", C.c_uint32), ("warp_task_max_len", C.c_uint32), ("cuckoo_max_chain", C.c_uint32),
+                ("cuckoo_max_attempts", C.c_uint32), ("reserved", C.c_uint32 * 2)]
 
 
 class Stats(C.Structure):
@@ -128,6 +130,8 @@ def lib():
         L.ptc_tensor_free.argtypes = [C.POINTER(Tensor)]
         L.ptc_tensor_free.restype = None
         L.ptc_device_count.restype = C.c_int
+        L.ptc_device_pool_in_use.argtypes = [C.c_int32, C.POINTER(C.c_uint64)]
+        L.ptc_device_pool_in_use.restype = C.c_int
         L.ptc_batch_contract.argtypes = [C.POINTER(BatchItem), C.c_uint32, C.POINTER(Options), C.POINTER(Tensor),
                                          SINK, C.c_void_p, C.POINTER(Stats)]
         L.ptc_batch_contract.restype = C.c_int
@@ -348,6 +352,13 @@ def batch_contract(items, *, outputs: str = "arrays", sink=None, **opt):
     if outputs == "device":
         return [outs[i] for i in range(n)], st.as_dict()
     return None, st.as_dict()
+
+
+def device_pool_in_use(device: int = -1) -> int:
+    """Bytes of the device's stream-ordered pool still allocated (ptc_device_pool_in_use)."""
+    v = C.c_uint64()
+    _check(lib().ptc_device_pool_in_use(device, C.byref(v)))
+    return int(v.value)
 
 
 def device_count() -> int:

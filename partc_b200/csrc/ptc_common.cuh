@@ -41,6 +41,22 @@ void set_last_error(ptc_status s, const std::string& msg);
         if (!(cond)) throw ::ptc::Error{(status), (message)};                                 \
     } while (0)
 
+// Restores the calling thread's current device when an entry point returns (entry points
+// switch to the device named in their options).
+class DeviceGuard {
+  public:
+    DeviceGuard() { ok_ = cudaGetDevice(&saved_) == cudaSuccess; }
+    ~DeviceGuard() {
+        if (ok_) cudaSetDevice(saved_);
+    }
+    DeviceGuard(const DeviceGuard&) = delete;
+    DeviceGuard& operator=(const DeviceGuard&) = delete;
+
+  private:
+    int saved_ = 0;
+    bool ok_ = false;
+};
+
 // ---- stream-ordered device arena ------------------------------------------------------------
 
 // Every device buffer of one call comes from here and is returned (stream-ordered) when the

@@ -46,6 +46,9 @@ constexpr uint32_t kDenseMinFraction = 5;
 constexpr uint64_t kEscMaxProducts = 256ull << 20;
 // largest per-fiber panel table (fibers x (panels + 1) offsets)
 constexpr uint64_t kPanelTableBytes = 4ull << 30;
+// cuckoo build of B's fibers: eviction chain bound and builds tried (ptc_options defaults)
+constexpr uint32_t kCuckooMaxChain = 64;
+constexpr uint32_t kCuckooMaxAttempts = 8;
 
 KeySpec make_keyspec(const uint32_t* dims, const uint32_t* modes, uint32_t n) {
     KeySpec k;
@@ -105,14 +108,13 @@ struct Events {
 
 enum { EV_START = 0, EV_H2D, EV_BSIDE, EV_ASIDE, EV_SYM, EV_NUM, EV_D2H, EV_WAVE0, EV_WAVE1 };
 
+// One non-blocking stream per device and host thread, kept for the thread's lifetime.
 cudaStream_t default_stream_for_thread(int device) {
-    thread_local int dev = -1;
-    thread_local cudaStream_t st = nullptr;
-    if (st == nullptr || dev != device) {
-        PTC_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-        dev = device;
-    }
-    return st;
+    constexpr int kMaxDevices = 64;
+    PTC_REQUIRE(device >= 0 && device < kMaxDevices, PTC_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+    thread_local cudaStream_t streams[kMaxDevices] = {};
+    if (!streams[device]) PTC_CUDA(cudaStreamCreateWithFlags(&streams[device], cudaStreamNonBlocking));
+    return streams[device];
 }
 
 // Keep freed stream-ordered allocations in the device's pool (instead of returning them to the
@@ -393,7 +395,8 @@ ptc_options resolve_options(const ptc_options* opt_in) {
     ptc_options opt;
     ptc_options_init(&opt);
     if (opt_in) {
-        PTC_REQUIRE(opt_in->struct_size >= offsetof(ptc_options, reserved), PTC_ERR_INVALID_ARGUMENT,
+        // callers built against the layout before the cuckoo fields get their defaults
+        PTC_REQUIRE(opt_in->struct_size >= offsetof(ptc_options, cuckoo_max_chain), PTC_ERR_INVALID_ARGUMENT,
                     "ptc_options.struct_size too small (call ptc_options_init)");
         std::memcpy(&opt, opt_in, std::min<size_t>(opt_in->struct_size, sizeof(opt)));
     }
@@ -571,9 +574,11 @@ struct Front {
 
 // Tuning knobs (the autotuner's search space), resolved from the options.
 struct Knobs {
-    uint32_t small_max;  // products of the largest row on the one-warp accumulator
-    uint32_t esc_avg;    // sort-based rows: fewer products per A nonzero than this on average
-    double max_load;     // cuckoo table load factor
+    uint32_t small_max;     // products of the largest row on the one-warp accumulator
+    uint32_t esc_avg;       // sort-based rows: fewer products per A nonzero than this on average
+    double max_load;        // cuckoo table load factor
+    uint32_t max_chain;     // cuckoo eviction chain bound
+    uint32_t max_attempts;  // cuckoo builds tried
 };
 
 Knobs knobs_of(const ptc_options& opt) {
@@ -581,6 +586,8 @@ Knobs knobs_of(const ptc_options& opt) {
     k.small_max = std::min(opt.small_max_products ? opt.small_max_products : kSmallMaxProducts, small_row_max_flops());
     k.esc_avg = opt.sort_max_avg_products ? opt.sort_max_avg_products : kEscMaxAvgProducts;
     k.max_load = opt.hash_load_pct ? std::min(std::max(opt.hash_load_pct, 10u), 90u) / 100.0 : 0.75;
+    k.max_chain = opt.cuckoo_max_chain;
+    k.max_attempts = opt.cuckoo_max_attempts ? opt.cuckoo_max_attempts : kCuckooMaxAttempts;
     return k;
 }
 
@@ -942,7 +949,7 @@ Front front_single(const ptc_coo* A, const ptc_coo* B, bool self, uint32_t c, co
     launch_tuples(dB.idx, dB.order, cols.run_start, cols.perm, ncols, b_free, col_tuple, st);
     Fibers fib = group_fibers(b_ckey, cols.rank_of, ncols, nb, bits_for_space(b_con.space), dB.vals, ar);
     CuckooBuildInfo cinfo;
-    const CuckooTable table = cuckoo_build(fib.key, fib.n, opt.hash_seed, 64, kn.max_load, 8, ar, &cinfo);
+    const CuckooTable table = cuckoo_build(fib.key, fib.n, opt.hash_seed, kn.max_chain, kn.max_load, kn.max_attempts, ar, &cinfo);
     stats.hash_attempts = cinfo.attempts;
     PTC_CUDA(cudaEventRecord(ev.ev[EV_BSIDE], st));
 
@@ -1329,7 +1336,7 @@ Front front_batch(const std::vector<BatchItemHost>& items, uint32_t location, co
     Fibers fib = group_fibers(b_ckey, cols.rank_of, cols.nruns, nb, bits_for_space((uint64_t)cb), b_vals, ar,
                               col_local);
     CuckooBuildInfo cinfo;
-    const CuckooTable table = cuckoo_build(fib.key, fib.n, opt.hash_seed, 64, kn.max_load, 8, ar, &cinfo);
+    const CuckooTable table = cuckoo_build(fib.key, fib.n, opt.hash_seed, kn.max_chain, kn.max_load, kn.max_attempts, ar, &cinfo);
     stats.hash_attempts = cinfo.attempts;
     PTC_CUDA(cudaEventRecord(ev.ev[EV_BSIDE], st));
     PTC_CUDA(cudaStreamSynchronize(st));  // h_col_first
@@ -1801,6 +1808,8 @@ void ptc_options_init(ptc_options* opt) {
     opt->path = PTC_PATH_TWO_PHASE;
     opt->output_location = PTC_HOST;
     opt->hash_seed = 0x243f6a8885a308d3ull;
+    opt->cuckoo_max_chain = ptc::kCuckooMaxChain;
+    opt->cuckoo_max_attempts = ptc::kCuckooMaxAttempts;
 }
 
 const char* ptc_status_string(ptc_status s) {
@@ -1815,7 +1824,6 @@ const char* ptc_status_string(ptc_status s) {
         case PTC_ERR_OUT_OF_MEMORY: return "PTC_ERR_OUT_OF_MEMORY";
         case PTC_ERR_CUDA: return "PTC_ERR_CUDA";
         case PTC_ERR_NO_DEVICE: return "PTC_ERR_NO_DEVICE";
-        case PTC_ERR_DEVICE_TIMEOUT: return "PTC_ERR_DEVICE_TIMEOUT";
         case PTC_ERR_OVERFLOW: return "PTC_ERR_OVERFLOW";
         case PTC_ERR_INTERNAL: return "PTC_ERR_INTERNAL";
     }
@@ -1829,6 +1837,7 @@ const char* ptc_last_error(void) {
 
 ptc_status ptc_contract(const ptc_coo* A, const ptc_coo* B, uint32_t c, const uint32_t* a_modes,
                         const uint32_t* b_modes, const ptc_options* opt, ptc_tensor* out, ptc_stats* stats) {
+    ptc::DeviceGuard keep_device;
     try {
         ptc::contract_impl(A, B, c, a_modes, b_modes, opt, out, stats);
         ptc::g_last_error.clear();
@@ -1848,6 +1857,7 @@ ptc_status ptc_contract(const ptc_coo* A, const ptc_coo* B, uint32_t c, const ui
 ptc_status ptc_sizer_collect(const ptc_coo* A, const ptc_coo* B, uint32_t c, const uint32_t* a_modes,
                              const uint32_t* b_modes, const ptc_options* opt, float** features, float** targets,
                              uint64_t* n) {
+    ptc::DeviceGuard keep_device;
     try {
         PTC_REQUIRE(features && targets && n, PTC_ERR_INVALID_ARGUMENT, "null output argument");
         ptc::Collect col;
@@ -1864,6 +1874,9 @@ ptc_status ptc_sizer_collect(const ptc_coo* A, const ptc_coo* B, uint32_t c, con
     } catch (const Error& e) {
         ptc::set_last_error(e.status, e.msg);
         return e.status;
+    } catch (const std::bad_alloc&) {
+        ptc::set_last_error(PTC_ERR_OUT_OF_MEMORY, "host allocation failed");
+        return PTC_ERR_OUT_OF_MEMORY;
     } catch (...) {
         ptc::set_last_error(PTC_ERR_INTERNAL, "unexpected exception");
         return PTC_ERR_INTERNAL;
@@ -1995,6 +2008,7 @@ extern "C" {
 ptc_status ptc_autotune(const ptc_batch_item* items, uint32_t n, const ptc_options* opt_in, uint32_t repeats,
                         ptc_options* best_out, ptc_tune_report* report) {
     using namespace ptc;
+    DeviceGuard keep_device;
     try {
         PTC_REQUIRE(best_out != nullptr && n > 0, PTC_ERR_INVALID_ARGUMENT, "need items and an output");
         ptc_options opt = resolve_options(opt_in);
@@ -2044,6 +2058,9 @@ ptc_status ptc_autotune(const ptc_batch_item* items, uint32_t n, const ptc_optio
     } catch (const Error& e) {
         set_last_error(e.status, e.msg);
         return e.status;
+    } catch (const std::bad_alloc&) {
+        set_last_error(PTC_ERR_OUT_OF_MEMORY, "host allocation failed");
+        return PTC_ERR_OUT_OF_MEMORY;
     } catch (...) {
         set_last_error(PTC_ERR_INTERNAL, "unexpected exception");
         return PTC_ERR_INTERNAL;
@@ -2053,6 +2070,7 @@ ptc_status ptc_autotune(const ptc_batch_item* items, uint32_t n, const ptc_optio
 ptc_status ptc_batch_contract(const ptc_batch_item* items, uint32_t n, const ptc_options* opt_in, ptc_tensor* outs,
                               ptc_batch_sink sink, void* user, ptc_stats* stats_out) {
     using namespace ptc;
+    DeviceGuard keep_device;
     try {
         const ptc_options opt = resolve_options(opt_in);
         PTC_REQUIRE(!opt.sort_rows, PTC_ERR_INVALID_ARGUMENT, "sort_rows is for single contractions");
@@ -2114,6 +2132,26 @@ void ptc_tensor_free(ptc_tensor* t) {
     t->vals = nullptr;
     t->opaque = nullptr;
     t->nnz = 0;
+}
+
+ptc_status ptc_device_pool_in_use(int32_t device, uint64_t* bytes) {
+    using namespace ptc;
+    DeviceGuard keep_device;
+    try {
+        PTC_REQUIRE(bytes != nullptr, PTC_ERR_INVALID_ARGUMENT, "bytes is null");
+        if (device < 0) PTC_CUDA(cudaGetDevice(&device));
+        PTC_CUDA(cudaSetDevice(device));
+        PTC_CUDA(cudaDeviceSynchronize());
+        cudaMemPool_t pool;
+        PTC_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+        uint64_t used = 0;
+        PTC_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used));
+        *bytes = used;
+        return PTC_OK;
+    } catch (const Error& e) {
+        set_last_error(e.status, e.msg);
+        return e.status;
+    }
 }
 
 int ptc_device_count(void) {

@@ -18,12 +18,14 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <new>
 #include <string>
 #include <vector>
 
 #include "partc.h"
 #include "ptc_build.cuh"
 #include "ptc_prims.cuh"
+#include "ptc_learned.cuh"
 
 namespace ptc {
 
@@ -201,6 +203,7 @@ uint32_t first_line_order(const char* buf, size_t n) {
 
 extern "C" ptc_status ptc_read_tns(const char* path, const ptc_options* opt_in, ptc_tensor* out, uint32_t* dims_out) {
     using namespace ptc;
+    DeviceGuard keep_device;
     std::vector<char> host;
     try {
         PTC_REQUIRE(path && out && dims_out, PTC_ERR_INVALID_ARGUMENT, "null argument");
@@ -242,10 +245,17 @@ extern "C" ptc_status ptc_read_tns(const char* path, const ptc_options* opt_in, 
         uint32_t* cnt = ar.alloc<uint32_t>(nchunks + 1);
         count_breaks_kernel<<<(unsigned)nchunks, 256, 0, st>>>(dbuf, n, cnt);
         PTC_CUDA(cudaGetLastError());
-        exclusive_scan<uint32_t>(cnt, cnt, nchunks, ar);
-        uint32_t nbreaks = 0;
-        PTC_CUDA(cudaMemcpyAsync(&nbreaks, cnt + nchunks, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        // the line positions below are 32-bit: count the breaks in 64 bits first and refuse files
+        // with 2^32 - 1 lines or more instead of wrapping
+        uint64_t* nbreaks64 = ar.alloc<uint64_t>(1);
+        launch_sum_u32(cnt, nchunks, nbreaks64, st);
+        uint64_t total_breaks = 0;
+        PTC_CUDA(cudaMemcpyAsync(&total_breaks, nbreaks64, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
         PTC_CUDA(cudaStreamSynchronize(st));
+        PTC_REQUIRE(total_breaks + 1 < (uint64_t)UINT32_MAX, PTC_ERR_INVALID_ARGUMENT,
+                    "the file has 2^32 - 1 lines or more");
+        exclusive_scan<uint32_t>(cnt, cnt, nchunks, ar);
+        const uint32_t nbreaks = (uint32_t)total_breaks;
         const uint64_t nlines = (uint64_t)nbreaks + 1;  // the text after the last break is a line too
         uint64_t* start = ar.alloc<uint64_t>(nlines + 1);
         line_starts_kernel<<<(unsigned)nchunks, 32, 0, st>>>(dbuf, n, cnt, start);
@@ -278,36 +288,48 @@ extern "C" ptc_status ptc_read_tns(const char* path, const ptc_options* opt_in, 
         double* oval = nullptr;
         PTC_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&oidx), std::max<uint64_t>((uint64_t)nnz * d, 1) * 4, st));
         PTC_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&oval), std::max<uint64_t>(nnz, 1) * 8, st));
+        // `out` owns the device arrays from here on, so every error path below releases them
+        out->location = PTC_DEVICE;
+        out->idx = oidx;
+        out->vals = oval;
+        out->order = d;
         compact_lines_kernel<<<grid, 256, 0, st>>>(tidx, tval, keep, pos, nlines, d, oidx, oval, dims);
         PTC_CUDA(cudaGetLastError());
         PTC_CUDA(cudaMemcpyAsync(dims_out, dims, d * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-        out->order = d;
-        out->nnz = nnz;
-        if (opt.output_location == PTC_DEVICE) {
-            out->location = PTC_DEVICE;
-            out->idx = oidx;
-            out->vals = oval;
-        } else {
-            out->location = PTC_HOST;
-            out->idx = static_cast<uint32_t*>(std::malloc(std::max<uint64_t>((uint64_t)nnz * d, 1) * 4));
-            out->vals = static_cast<double*>(std::malloc(std::max<uint64_t>(nnz, 1) * 8));
-            if (!out->idx || !out->vals) {
-                cudaFreeAsync(oidx, st);
-                cudaFreeAsync(oval, st);
+        if (opt.output_location != PTC_DEVICE) {
+            uint32_t* hidx = static_cast<uint32_t*>(std::malloc(std::max<uint64_t>((uint64_t)nnz * d, 1) * 4));
+            double* hval = static_cast<double*>(std::malloc(std::max<uint64_t>(nnz, 1) * 8));
+            if (!hidx || !hval) {
+                std::free(hidx);
+                std::free(hval);
                 throw Error{PTC_ERR_OUT_OF_MEMORY, "host allocation failed"};
             }
-            PTC_CUDA(cudaMemcpyAsync(out->idx, oidx, (uint64_t)nnz * d * 4, cudaMemcpyDeviceToHost, st));
-            PTC_CUDA(cudaMemcpyAsync(out->vals, oval, (uint64_t)nnz * 8, cudaMemcpyDeviceToHost, st));
-            PTC_CUDA(cudaFreeAsync(oidx, st));
-            PTC_CUDA(cudaFreeAsync(oval, st));
+            const cudaError_t e1 = cudaMemcpyAsync(hidx, oidx, (uint64_t)nnz * d * 4, cudaMemcpyDeviceToHost, st);
+            const cudaError_t e2 = cudaMemcpyAsync(hval, oval, (uint64_t)nnz * 8, cudaMemcpyDeviceToHost, st);
+            const cudaError_t e3 = cudaStreamSynchronize(st);
+            if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
+                std::free(hidx);
+                std::free(hval);
+                PTC_CUDA(e1 != cudaSuccess ? e1 : e2 != cudaSuccess ? e2 : e3);
+            }
+            cudaFreeAsync(oidx, st);
+            cudaFreeAsync(oval, st);
+            out->location = PTC_HOST;
+            out->idx = hidx;
+            out->vals = hval;
         }
         ar.release();
         PTC_CUDA(cudaStreamSynchronize(st));
+        out->nnz = nnz;
         return PTC_OK;
     } catch (const Error& e) {
         ptc_tensor_free(out);
         set_last_error(e.status, e.msg);
         return e.status;
+    } catch (const std::bad_alloc&) {
+        ptc_tensor_free(out);
+        set_last_error(PTC_ERR_OUT_OF_MEMORY, "host allocation failed");
+        return PTC_ERR_OUT_OF_MEMORY;
     } catch (...) {
         ptc_tensor_free(out);
         set_last_error(PTC_ERR_INTERNAL, "unexpected exception");
@@ -348,5 +370,11 @@ extern "C" ptc_status ptc_write_tns(const char* path, const ptc_tensor* t) {
     } catch (const Error& e) {
         set_last_error(e.status, e.msg);
         return e.status;
+    } catch (const std::bad_alloc&) {
+        set_last_error(PTC_ERR_OUT_OF_MEMORY, "host allocation failed");
+        return PTC_ERR_OUT_OF_MEMORY;
+    } catch (...) {
+        set_last_error(PTC_ERR_INTERNAL, "unexpected exception");
+        return PTC_ERR_INTERNAL;
     }
 }

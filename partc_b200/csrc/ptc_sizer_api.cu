@@ -12,6 +12,7 @@ namespace ptc {
 namespace {
 
 constexpr char kMagic[8] = {'P', 'T', 'C', 'S', 'Z', 'R', '0', '1'};
+constexpr int kMaxStreamDevices = 64;
 
 cudaStream_t sizer_stream(int32_t device) {
     int ndev = 0;
@@ -20,19 +21,18 @@ cudaStream_t sizer_stream(int32_t device) {
         throw Error{PTC_ERR_NO_DEVICE, "no usable CUDA device"};
     }
     if (device >= 0) PTC_CUDA(cudaSetDevice(device));
-    thread_local cudaStream_t st = nullptr;
-    thread_local int dev = -1;
     int cur = 0;
     PTC_CUDA(cudaGetDevice(&cur));
-    if (!st || dev != cur) {
-        PTC_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-        dev = cur;
-    }
-    return st;
+    PTC_REQUIRE(cur < kMaxStreamDevices, PTC_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+    // one stream per device and host thread, kept for the thread's lifetime
+    thread_local cudaStream_t streams[kMaxStreamDevices] = {};
+    if (!streams[cur]) PTC_CUDA(cudaStreamCreateWithFlags(&streams[cur], cudaStreamNonBlocking));
+    return streams[cur];
 }
 
 template <typename F>
 ptc_status guarded(F&& f) {
+    DeviceGuard keep_device;
     try {
         f();
         return PTC_OK;

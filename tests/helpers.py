@@ -30,3 +30,41 @@ def load_golden(path):
     z = np.load(path)
     t = CooTensor(idx=z["idx"], vals=z["vals"], dims=z["dims"])
     return t, int(z["c"]), [int(x) for x in z["modes"]], z["out_idx"], z["out_vals"]
+
+
+def digest(idx, vals):
+    """sha256 of an output tensor in canonical order (index tuples, then value bits)."""
+    import hashlib
+    ci, cv = canonical(np.ascontiguousarray(idx, dtype=np.uint32), np.ascontiguousarray(vals, dtype=np.float64))
+    h = hashlib.sha256()
+    h.update(np.ascontiguousarray(ci).tobytes())
+    h.update(np.ascontiguousarray(cv).view(np.uint64).tobytes())
+    return h.hexdigest()
+
+
+def input_digest(t):
+    """sha256 of a generated COO tensor (indices, values, mode sizes)."""
+    import hashlib
+    h = hashlib.sha256()
+    for a in (t.idx, t.vals, t.dims):
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+def free_keys(t, modes):
+    """Linearized key of every nonzero over the given modes (first mode most significant)."""
+    k = np.zeros(t.nnz, dtype=np.uint64)
+    for m in modes:
+        k = k * np.uint64(t.dims[m]) + t.idx[:, m].astype(np.uint64)
+    return k
+
+
+def sample_rows(row_keys, row_nnz, n_top=10, n_random=1000, seed=20):
+    """Row keys of a seeded sample: the n_top rows with the most output entries and n_random
+    other rows drawn uniformly."""
+    order = np.argsort(-row_nnz.astype(np.int64), kind="stable")
+    top = order[:n_top]
+    rest = order[n_top:]
+    rng = np.random.default_rng(seed)
+    pick = rng.choice(rest, size=min(n_random, rest.size), replace=False)
+    return np.sort(row_keys[np.concatenate([top, pick])])
