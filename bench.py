@@ -37,6 +37,9 @@ sys.path.insert(0, ROOT)
 
 WORKLOAD = "zipf4d_3m"
 FALLBACK_HBM_GBS = 6650.0
+TUNE_SEED = 1001    # the autotuner's held-out tensor: the timed workload drawn with this seed
+CPU_WARMUP = 1      # reference runs before the timed ones (both CPU legs)
+CPU_STEPS = 3       # timed reference runs of the cpu_baseline leg (median)
 
 
 class ClockSampler:
@@ -84,6 +87,25 @@ class ClockSampler:
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def host_info():
+    """The host's core count, CPU model and memory (for the CPU baselines)."""
+    info = {"nproc": os.cpu_count(), "cpu_model": None, "ram_gb": None}
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    info["cpu_model"] = line.split(":", 1)[1].strip()
+                    break
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemTotal"):
+                    info["ram_gb"] = round(int(line.split()[1]) / 1024 ** 2, 1)
+                    break
+    except OSError:
+        pass
+    return info
 
 
 def measured_hbm_peak():
@@ -154,11 +176,18 @@ def run_port_once(w, keep):
 
 
 def cpu_arm(w, target_flops, steps, warmup):
-    """Times the reference (or the port) on a row sample; returns (value, cpu_baseline dict)."""
+    """Times the reference (or the port) on a row sample; returns (value, cpu_baseline dict).
+
+    The sample is seeded (the same rows for the reference arm and the cpu_baseline leg of the GPU
+    arm).  value = the sample's mult-adds over the median time of the reference's whole path
+    (HT_B and HT_A builds over the whole B and the sampled rows, preprocessing, numeric pass);
+    numeric_only = the same mult-adds over the median of the reference's own "Total time for
+    tensor contraction" line (fksCuckooTC.hpp:362-365), which excludes the builds that do not
+    shrink with the sample."""
     import oracle
     keep, sflops, nrows = _row_sample(w, target_flops)
     kind = "reference" if os.path.exists(oracle.REF_BIN) else "port"
-    times = []
+    times, numeric = [], []
     with tempfile.TemporaryDirectory() as td:
         for i in range(warmup + steps):
             if kind == "reference":
@@ -167,17 +196,35 @@ def cpu_arm(w, target_flops, steps, warmup):
                 r = run_port_once(w, keep)
             if i >= warmup:
                 times.append(r["t_wall"])
+                if r.get("t_contract"):
+                    numeric.append(r["t_contract"])
     t = statistics.median(times)
     value = sflops / t
     # the reference is offered every host core (OMP_NUM_THREADS), but its hash builds are serial
     # loops and its numeric loop runs a team of one (fksCuckooTC.hpp:171-173): one core works
     cores = 1
-    sample = (f"{nrows} of A's rows (whole rows, seeded) against the whole B: {sflops} mult-adds; time = the "
-              f"reference's HT_B + HT_A builds, preprocessing and numeric pass; median of {len(times)}; "
+    sample = (f"{nrows} of A's rows (whole rows, seeded) against the whole B: {sflops} mult-adds "
+              f"({100.0 * sflops / max(1, w_flops(w)):.2f}% of the workload's); time = the reference's HT_B + "
+              f"HT_A builds, preprocessing and numeric pass; median of {len(times)} after {warmup} warm-up; "
               f"OMP_NUM_THREADS={os.cpu_count()} offered, the reference's loops use one thread "
               f"(fksCuckooTC.hpp:171-173)")
-    return value, {"value": value, "unit": "mult-adds/s", "cores": cores, "kind": kind, "sample": sample,
-                   "sample_mult_adds": sflops, "seconds": t}
+    out = {"value": value, "unit": "mult-adds/s", "cores": cores, "kind": kind, "sample": sample,
+           "sample_mult_adds": sflops, "seconds": t, "host": host_info()}
+    if numeric:
+        out["numeric_only"] = {"value": sflops / statistics.median(numeric), "unit": "mult-adds/s",
+                               "seconds": statistics.median(numeric)}
+    return value, out
+
+
+_FLOPS_CACHE = {}
+
+
+def w_flops(w):
+    """Mult-adds of the whole workload (the oracle's flop count, cached)."""
+    import oracle
+    if w.name not in _FLOPS_CACHE:
+        _FLOPS_CACHE[w.name] = int(oracle.contract(w.tensor, None, w.c, w.modes, mode=oracle.FLOPS_ONLY)["flops"])
+    return _FLOPS_CACHE[w.name]
 
 
 def cpu_arm_batch(n_items, target_seconds, steps, warmup):
@@ -409,6 +456,56 @@ def run_batch(args, rank, world, local):
         print(json.dumps(line))
 
 
+def batch_record(n, local, stream, steps, warmup=1):
+    """The first n members of the uneven batch (gen.batch_member seeds 0..n-1) through
+    ptc_batch_contract on both paths, inputs resident in HBM, outputs produced wave by wave and
+    discarded; CUDA events on the library's stream.  A record for the default bench line."""
+    import torch
+    from partc_b200 import _lib, gen
+    work = gen.batch_members(n, procs=min(16, os.cpu_count() or 1))
+    dev = f"cuda:{local}"
+    idx_cat = np.concatenate([w.tensor.idx.reshape(-1) for w in work]).view(np.int32)
+    val_cat = np.concatenate([w.tensor.vals for w in work])
+    di = torch.from_numpy(idx_cat).to(dev)
+    dv = torch.from_numpy(val_cat).to(dev)
+    keep = []
+    items = (_lib.BatchItem * n)()
+    io = vo = 0
+    for i, w in enumerate(work):
+        t = w.tensor
+        items[i].A = _lib.device_coo(di.data_ptr() + 4 * io, dv.data_ptr() + 8 * vo, t.nnz, t.dims, keep)
+        items[i].c = w.c
+        for j, m in enumerate(w.modes):
+            items[i].a_modes[j] = m
+        io += t.nnz * t.order
+        vo += t.nnz
+    rec = {"items": n, "nnz": int(vo), "seeds": f"0..{n - 1}"}
+    for path in ("two_phase", "learned"):
+        opts = dict(device=local, stream=stream.cuda_stream, path=path)
+        for _ in range(warmup):
+            _, st = _lib.batch_contract(items, outputs="none", **opts)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        sts = []
+        e0.record(stream)
+        for _ in range(steps):
+            sts.append(_lib.batch_contract(items, outputs="none", **opts)[1])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        M = sts[0]["mult_adds"]
+        rec[path] = {"value": M / (ms * 1e-3), "unit": "mult-adds/s", "ms_per_step": ms, "mult_adds": M,
+                     "out_nnz": sts[0]["out_nnz"], "rerun_items": int(sts[0]["rerun_items"]),
+                     "t_symbolic_ms": statistics.mean(x["t_symbolic_ms"] for x in sts),
+                     "t_numeric_ms": statistics.mean(x["t_numeric_ms"] for x in sts),
+                     "launches_per_step": int(sts[0]["kernel_launches"])}
+    rec["learned_over_two_phase"] = rec["learned"]["value"] / rec["two_phase"]["value"]
+    del di, dv
+    torch.cuda.empty_cache()
+    return rec
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -419,17 +516,22 @@ def main():
     ap.add_argument("--no-compare-paths", dest="compare_paths", action="store_false")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false")
     ap.add_argument("--workload", default=WORKLOAD)
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-target-flops", type=float, default=6e7)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-items", type=int, default=4096)
     ap.add_argument("--batch-path", default="two_phase", choices=["two_phase", "learned"])
     ap.add_argument("--no-cusparse", dest="cusparse", action="store_false")
     ap.add_argument("--no-per-contraction", dest="per_contraction", action="store_false")
+    ap.add_argument("--batch-record", type=int, default=256,
+                    help="members of the uneven batch timed on both paths for the default line (0: none)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
     from partc_b200 import dist as pdist
+    if pdist.needs_launcher(args.gpus):
+        # one replica rank per GPU: start this script again under the launcher
+        sys.exit(subprocess.call(pdist.launcher_command(os.path.abspath(__file__), sys.argv[1:], args.gpus)))
     rank, world, local = pdist.rank_env()
 
     if args.workload.startswith("batch") and args.impl == "ours":
@@ -464,14 +566,15 @@ def main():
         if not pdist.runs_reference_arm(rank):
             return
         steps = max(1, args.steps)
-        value, cb = cpu_arm(w, int(args.cpu_target_flops / 2), steps, min(args.warmup, 1))
+        value, cb = cpu_arm(w, int(args.cpu_target_flops), steps, CPU_WARMUP)
         line = {"impl": "reference", "metric": "contraction mult-adds/s", "value": value, "unit": "mult-adds/s",
-                "n_gpus": args.gpus, "steps": steps, "warmup": min(args.warmup, 1), "ms_per_step": cb["seconds"] * 1e3,
+                "n_gpus": args.gpus, "steps": steps, "warmup": CPU_WARMUP, "ms_per_step": cb["seconds"] * 1e3,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded generator, partc_b200/gen.py)",
                 "config": {"workload": w.name, "nnz": t.nnz, "dims": [int(x) for x in t.dims], "contracted_modes":
                            w.modes[:w.c], "parallelism": "host cores"},
-                "cpu_baseline": {k: cb[k] for k in ("kind", "cores", "sample", "value")},
+                "cpu_baseline": {k: cb[k] for k in ("kind", "cores", "sample", "value", "numeric_only", "host")
+                                 if k in cb},
                 "e2e": {"value": value, "unit": "mult-adds/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
@@ -490,16 +593,26 @@ def main():
     keep = []
     coo = _lib.device_coo(di.data_ptr(), dv.data_ptr(), t.nnz, t.dims, keep)
     opts = dict(output_location="device", device=local, stream=stream.cuda_stream, path=args.path)
-    knobs = {}
-    if args.autotune:  # the library's autotuner picks the knobs on this workload (untimed)
+    tuned = {args.path: {}}
+    other = "two_phase" if args.path == "learned" else "learned"
+    if args.autotune:
+        # the library's autotuner picks each path's knobs (untimed) on a held-out tensor: the same
+        # workload drawn with another seed, never the tensor that is timed
+        wt = gen.WORKLOADS[args.workload](seed=TUNE_SEED)
+        ti = torch.from_numpy(wt.tensor.idx.view(np.int32)).to(f"cuda:{local}")
+        tv = torch.from_numpy(wt.tensor.vals).to(f"cuda:{local}")
         items = (_lib.BatchItem * 1)()
-        items[0].A = coo
-        items[0].c = w.c
-        for j, m in enumerate(w.modes):
+        items[0].A = _lib.device_coo(ti.data_ptr(), tv.data_ptr(), wt.tensor.nnz, wt.tensor.dims, keep)
+        items[0].c = wt.c
+        for j, m in enumerate(wt.modes):
             items[0].a_modes[j] = m
-        knobs, tune = _lib.autotune(items, repeats=1, device=local, stream=stream.cuda_stream, path=args.path)
-        knobs = {k: v for k, v in knobs.items() if v}
-        opts.update(knobs)
+        for p in ([args.path, other] if args.compare_paths else [args.path]):
+            kn, _ = _lib.autotune(items, repeats=1, device=local, stream=stream.cuda_stream, path=p)
+            tuned[p] = {k: v for k, v in kn.items() if v}
+        del ti, tv, items
+        torch.cuda.empty_cache()
+    knobs = tuned[args.path]
+    opts.update(knobs)
 
     def step():
         out, st = _lib.contract_coo(coo, None, w.c, w.modes, **opts)
@@ -528,14 +641,15 @@ def main():
     value = pdist.job_throughput(M, args.steps, world, ms * 1e-3)
     ms_step = ms / args.steps
 
-    # the other path, timed the same way (learned-sized against exact two-phase sizing)
-    other = "two_phase" if args.path == "learned" else "learned"
+    # the other path, timed the same way (learned-sized against exact two-phase sizing), with the
+    # knobs tuned for it
     paths = {args.path: {"value": value, "ms_per_step": ms_step,
                          "t_symbolic_ms": statistics.mean(s["t_symbolic_ms"] for s in stats),
                          "rerun_rows": int(stats[0]["rerun_rows"]),
                          "sizer_mean_abs_log2_err": stats[0]["sizer_mean_abs_log2_err"]}}
     if args.compare_paths:
-        oopts = dict(opts, path=other)
+        oopts = dict(output_location="device", device=local, stream=stream.cuda_stream, path=other,
+                     **tuned.get(other, {}))
         for _ in range(2):
             out, _ = _lib.contract_coo(coo, None, w.c, w.modes, **oopts)
             _lib.free(out)
@@ -554,7 +668,8 @@ def main():
                         "ms_per_step": oms / args.steps,
                         "t_symbolic_ms": statistics.mean(s["t_symbolic_ms"] for s in ost),
                         "rerun_rows": int(ost[0]["rerun_rows"]),
-                        "sizer_mean_abs_log2_err": ost[0]["sizer_mean_abs_log2_err"]}
+                        "sizer_mean_abs_log2_err": ost[0]["sizer_mean_abs_log2_err"],
+                        "knobs": tuned.get(other) or "defaults"}
 
     # numeric pass roofline
     od = 2 * (t.order - w.c)
@@ -590,11 +705,14 @@ def main():
                "steps": args.e2e_steps, "ms_per_step": el / args.e2e_steps * 1e3}
 
     cusparse = matricized_cusparse(w, f"cuda:{local}", M) if (args.cusparse and rank == 0 and world == 1) else None
+    batch = None
+    if args.batch_record > 0 and rank == 0 and world == 1:
+        batch = batch_record(args.batch_record, local, stream, steps=3)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            _, cpu = cpu_arm(w, int(args.cpu_target_flops), 1, 0)
+            _, cpu = cpu_arm(w, int(args.cpu_target_flops), CPU_STEPS, CPU_WARMUP)
         except Exception as ex:  # reported, never fatal to the GPU number
             cpu = {"value": None, "error": str(ex)[:200]}
 
@@ -614,7 +732,7 @@ def main():
                          ("t_build_ms", "t_symbolic_ms", "t_numeric_ms", "t_total_ms")},
             "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
             "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clk.summary(),
-            "matricized_cusparse": cusparse, "paths": paths,
+            "matricized_cusparse": cusparse, "paths": paths, f"batch{args.batch_record}": batch,
         }
         print(json.dumps(line))
     if world > 1:

@@ -24,9 +24,17 @@ REF_BIN = os.path.join(HERE, "_ref", "ref_tc")
 FLOPS_ONLY, COUNTS, VALUES = 0, 1, 2
 
 
-def build(ref: str = "/root/reference") -> None:
+def reference_dir(ref: Optional[str] = None) -> str:
+    """Where the reference's sources are: the argument, else the environment variable
+    ``PARTC_REFERENCE``, else a checkout named ``reference`` beside this repository."""
+    if ref:
+        return ref
+    return os.environ.get("PARTC_REFERENCE") or os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
+
+
+def build(ref: Optional[str] = None) -> None:
     """Compile the restatement and, where the reference sources exist, ``oracle/_ref``."""
-    subprocess.run(["make", "-s", "-C", HERE, f"REF={ref}"], check=True)
+    subprocess.run(["make", "-s", "-C", HERE, f"REF={reference_dir(ref)}"], check=True)
 
 
 class _Coo(C.Structure):

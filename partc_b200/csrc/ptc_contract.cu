@@ -11,6 +11,9 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <unistd.h>
+#include <unordered_map>
+#include <map>
 
 #include <dlfcn.h>
 #include <sys/mman.h>
@@ -358,6 +361,106 @@ HostCopier& host_copier() {
     return c;
 }
 
+// Pinned host blocks for results, kept between calls.  A result copied into pinned memory goes
+// from HBM to the host by DMA at the link's speed, with no staging copy; pinning fresh memory for
+// every call would cost more than the copy itself, so released blocks wait here for the next
+// result of a similar size.  At most `cap` bytes are kept (environment variable
+// PARTC_PINNED_POOL_MIB; default a quarter of the host's memory; 0 turns the pool off).
+class PinnedPool {
+  public:
+    static PinnedPool& get() {
+        static PinnedPool* p = new PinnedPool;  // never destroyed: blocks may outlive static teardown
+        return *p;
+    }
+    // A block of at least `bytes` bytes, or nullptr (pool off, or the allocation failed).
+    void* take(size_t bytes) {
+        if (cap_ == 0 || bytes < kMinBytes) return nullptr;
+        const size_t want = round_up(bytes);
+        {
+            std::lock_guard<std::mutex> lock(mu_);
+            auto it = free_.lower_bound(want);
+            if (it != free_.end() && it->first <= 2 * want) {
+                void* p = it->second;
+                kept_ -= it->first;
+                free_.erase(it);
+                return p;
+            }
+        }
+        void* p = nullptr;
+        if (cudaHostAlloc(&p, want, cudaHostAllocPortable) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        std::lock_guard<std::mutex> lock(mu_);
+        size_[p] = want;
+        return p;
+    }
+    // Back to the pool (the oldest kept blocks are freed while the pool holds more than cap).
+    void give(void* p) {
+        if (!p) return;
+        std::vector<void*> drop;
+        {
+            std::lock_guard<std::mutex> lock(mu_);
+            const size_t sz = size_.at(p);
+            free_.emplace(sz, p);
+            kept_ += sz;
+            while (kept_ > cap_ && !free_.empty()) {
+                auto it = free_.begin();
+                kept_ -= it->first;
+                drop.push_back(it->second);
+                size_.erase(it->second);
+                free_.erase(it);
+            }
+        }
+        for (void* q : drop) cudaFreeHost(q);
+    }
+
+  private:
+    static constexpr size_t kMinBytes = 64ull << 20;  // smaller results take the plain path
+    static constexpr size_t kRound = 64ull << 20;
+    static size_t round_up(size_t b) { return (b + kRound - 1) / kRound * kRound; }
+    PinnedPool() {
+        const char* env = std::getenv("PARTC_PINNED_POOL_MIB");
+        if (env) {
+            cap_ = (size_t)std::strtoull(env, nullptr, 10) << 20;
+        } else {
+            const long pages = sysconf(_SC_PHYS_PAGES), page = sysconf(_SC_PAGE_SIZE);
+            cap_ = (pages > 0 && page > 0) ? (size_t)pages * (size_t)page / 4 : 0;
+        }
+    }
+    std::mutex mu_;
+    std::multimap<size_t, void*> free_;        // kept blocks by size
+    std::unordered_map<void*, size_t> size_;   // size of every block the pool made
+    size_t kept_ = 0;
+    size_t cap_ = 0;
+};
+
+// Output block behind a ptc_tensor's arrays (ptc_tensor::opaque): one wave of a batch, shared by
+// the item tensors cut from it, or a single result in pinned pool blocks.  The last
+// ptc_tensor_free of its tensors releases it.
+constexpr uint32_t kPinnedPoolBlock = 2;  // location of a block from the pinned pool
+struct SharedBlock {
+    std::atomic<uint32_t> refs{0};
+    uint32_t location = PTC_HOST;  // PTC_HOST (malloc), PTC_DEVICE, or kPinnedPoolBlock
+    void* idx = nullptr;
+    void* val = nullptr;
+};
+
+void release_block(SharedBlock* b) {
+    if (b->refs.fetch_sub(1) != 1) return;
+    if (b->location == PTC_DEVICE) {
+        cudaFree(b->idx);
+        cudaFree(b->val);
+    } else if (b->location == kPinnedPoolBlock) {
+        PinnedPool::get().give(b->idx);
+        PinnedPool::get().give(b->val);
+    } else {
+        std::free(b->idx);
+        std::free(b->val);
+    }
+    delete b;
+}
+
 void print_reference_lines(const ptc_stats& s) {
     // the reference's stdout lines (fksCuckoo.hpp:1056-1057, fksCuckooTC.hpp:161,364-365)
     printf("Number of elements inserted = %llu\n", (unsigned long long)s.b_nnz);
@@ -570,6 +673,12 @@ struct Front {
     std::vector<uint32_t> h_row_first;    // host copy
     std::vector<uint32_t> colbase;        // first global column of each item (nitems + 1 entries)
     ItemOut* item_out = nullptr;          // device [nitems], filled per wave
+    // per-item statistics for the sizer's features (batches; device arrays)
+    const uint64_t* b_off = nullptr;      // [nitems + 1] first B nonzero of each item
+    const uint32_t* col_first = nullptr;  // [nitems + 1] first global column
+    const uint32_t* fib_first = nullptr;  // [nitems + 1] first fiber
+    const uint32_t* col_run = nullptr;    // [global columns + 1] B nonzeros before each column
+    uint64_t ncols_global = 0;
 };
 
 // Tuning knobs (the autotuner's search space), resolved from the options.
@@ -720,8 +829,6 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
     // that each fit one shared-memory table (W <= table capacity, so a part always fits).  The
     // per-fiber panel table is built when it fits kPanelTableBytes (else binary searches in the
     // fiber find a part's entries).
-    PTC_REQUIRE(ncols <= sym_bitmap_max_cols(), PTC_ERR_INVALID_ARGUMENT,
-                "more than 1.5M distinct B free keys in one contraction is not supported yet");
     auto table_bytes = [&](uint32_t w) { return nfib * ((ncols + w - 1) / w + 1) * 4; };
     uint32_t W = opt.panel_width;
     // a batch's large rows each have their own item's panels: per-row panel counts
@@ -854,14 +961,41 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
         PTC_CUDA(cudaMemsetAsync(pl.claim_off, 0, (nrows + 1) * sizeof(uint64_t), st));
         if (n_big > 0) {
             // sizer: per-row features -> predicted log2(1 + nnz) -> per-panel counts by column popularity
-            float* gp = ar.alloc<float>((uint64_t)(P + 1) * kGridPoints);
-            launch_popularity_table(op.b_col, nb, ncols, P, pl.log2w, gp, ar);
+            // (a batch uses its items' own tables below instead of one over the whole batch)
+            float* gp = nullptr;
+            if (!F.batch) {
+                gp = ar.alloc<float>((uint64_t)(P + 1) * kGridPoints);
+                launch_popularity_table(op.b_col, nb, ncols, P, pl.log2w, gp, ar);
+            }
+            // a batch row gets its own item's statistics (the features a single contraction of
+            // that item gives, which the sizer was trained on)
+            ItemStats is;
+            if (F.batch) {
+                is.nitems = F.nitems;
+                is.b_off = F.b_off;
+                is.col_first = F.col_first;
+                is.fib_first = F.fib_first;
+                is.row_first = F.row_first;
+                is.col_run = F.col_run;
+                is.gtot = ar.alloc<float>((uint64_t)F.nitems * kGridPoints);
+                std::vector<uint64_t> ipb(F.nitems + 1, 0);
+                for (uint32_t i = 0; i < F.nitems; ++i)
+                    ipb[i + 1] = ipb[i] + std::max<uint64_t>(1, (item_cols_h[i] + W - 1) / W);
+                uint64_t* ipb_d = ar.alloc<uint64_t>(F.nitems + 1);
+                PTC_CUDA(cudaMemcpyAsync(ipb_d, ipb.data(), ipb.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+                is.item_pb = ipb_d;
+                is.pmass = ar.alloc<uint32_t>(std::max<uint64_t>(ipb[F.nitems], 1));
+                PTC_CUDA(cudaMemsetAsync(is.pmass, 0, std::max<uint64_t>(ipb[F.nitems], 1) * sizeof(uint32_t), st));
+                launch_item_popularity(is, F.ncols_global, pl.log2w, ar);
+                PTC_CUDA(cudaStreamSynchronize(st));  // ipb (host) stays alive until the copy is done
+            }
             float* fx = ar.alloc<float>((uint64_t)n_big * kSizerInputs);
-            launch_row_features(op, pl.big_rows, n_big, pl.row_flops, gp, fx, st);
+            launch_row_features(op, pl.big_rows, n_big, pl.row_flops, gp, fx, st, F.batch ? &is : nullptr);
             pl.pred = ar.alloc<float>(n_big);
             sizer_predict_device(*sizer, fx, n_big, pl.pred, ar);
             launch_predicted_panel_counts(pl.big_rows, n_big, pl.row_flops, pl.pred, gp, op.row_item, item_cols,
-                                          pbase, P, pl.log2w, ncols, kSizerMargin, panel_cnt, ar);
+                                          pbase, P, pl.log2w, ncols, kSizerMargin, panel_cnt, ar,
+                                          F.batch ? &is : nullptr);
             launch_claim_budgets(pl.big_rows, n_big, panel_cnt, pbase, P, pl.claim_off, st);
         }
         exclusive_scan<uint64_t>(pl.claim_off, pl.claim_off, nrows, ar);
@@ -1114,19 +1248,37 @@ void contract_impl(const ptc_coo* A, const ptc_coo* Bin, uint32_t c, const uint3
         PTC_CUDA(cudaEventRecord(ev.ev[EV_D2H], st));
     } else {
         out->location = PTC_HOST;
-        out->idx = static_cast<uint32_t*>(host_result_alloc(out_nnz * od * sizeof(uint32_t)));
-        out->vals = static_cast<double*>(host_result_alloc(out_nnz * sizeof(double)));
-        if (!out->idx || !out->vals) {
-            std::free(out->idx);
-            std::free(out->vals);
-            cudaFreeAsync(ov.idx, st);
-            cudaFreeAsync(ov.val, st);
-            out->idx = nullptr;
-            out->vals = nullptr;
-            throw Error{PTC_ERR_OUT_OF_MEMORY, "host output allocation failed"};
+        const size_t ib = out_nnz * od * sizeof(uint32_t), vb = out_nnz * sizeof(double);
+        void* pi = PinnedPool::get().take(ib);
+        void* pv = pi ? PinnedPool::get().take(vb) : nullptr;
+        if (pi && pv) {
+            // pinned pool blocks: one DMA per array, no staging
+            SharedBlock* blk = new SharedBlock;
+            blk->refs = 1;
+            blk->location = kPinnedPoolBlock;
+            blk->idx = pi;
+            blk->val = pv;
+            out->opaque = blk;
+            out->idx = static_cast<uint32_t*>(pi);
+            out->vals = static_cast<double*>(pv);
+            PTC_CUDA(cudaMemcpyAsync(pi, ov.idx, ib, cudaMemcpyDeviceToHost, st));
+            PTC_CUDA(cudaMemcpyAsync(pv, ov.val, vb, cudaMemcpyDeviceToHost, st));
+        } else {
+            if (pi) PinnedPool::get().give(pi);
+            out->idx = static_cast<uint32_t*>(host_result_alloc(ib));
+            out->vals = static_cast<double*>(host_result_alloc(vb));
+            if (!out->idx || !out->vals) {
+                std::free(out->idx);
+                std::free(out->vals);
+                cudaFreeAsync(ov.idx, st);
+                cudaFreeAsync(ov.val, st);
+                out->idx = nullptr;
+                out->vals = nullptr;
+                throw Error{PTC_ERR_OUT_OF_MEMORY, "host output allocation failed"};
+            }
+            host_copier().copy(out->idx, ov.idx, ib, st);
+            host_copier().copy(out->vals, ov.val, vb, st);
         }
-        host_copier().copy(out->idx, ov.idx, out_nnz * od * sizeof(uint32_t), st);
-        host_copier().copy(out->vals, ov.val, out_nnz * sizeof(double), st);
         PTC_CUDA(cudaFreeAsync(ov.idx, st));
         PTC_CUDA(cudaFreeAsync(ov.val, st));
         PTC_CUDA(cudaEventRecord(ev.ev[EV_D2H], st));
@@ -1158,27 +1310,6 @@ void contract_impl(const ptc_coo* A, const ptc_coo* Bin, uint32_t c, const uint3
 // index tables by them); the items' rows are contiguous in row order.  The output of the batch is
 // produced in waves of consecutive items whose outputs fit a device budget; each wave's numeric
 // pass is one CUDA-graph launch.
-
-// Output block of one wave, shared by the item tensors cut from it (ptc_tensor::opaque); the last
-// ptc_tensor_free of them releases it.
-struct SharedBlock {
-    std::atomic<uint32_t> refs{0};
-    uint32_t location = PTC_HOST;
-    void* idx = nullptr;
-    void* val = nullptr;
-};
-
-void release_block(SharedBlock* b) {
-    if (b->refs.fetch_sub(1) != 1) return;
-    if (b->location == PTC_DEVICE) {
-        cudaFree(b->idx);
-        cudaFree(b->val);
-    } else {
-        std::free(b->idx);
-        std::free(b->val);
-    }
-    delete b;
-}
 
 struct BatchItemHost {
     const ptc_coo* A;
@@ -1335,6 +1466,12 @@ Front front_batch(const std::vector<BatchItemHost>& items, uint32_t location, co
     launch_item_tuples(cols.run_start, cols.perm, cols.nruns, specs_d, b_off_d, n, 1, fb_w, col_tuple, st);
     Fibers fib = group_fibers(b_ckey, cols.rank_of, cols.nruns, nb, bits_for_space((uint64_t)cb), b_vals, ar,
                               col_local);
+    // each item's fibers are contiguous (its contracted keys start at its cbase)
+    std::vector<uint64_t> cbase_h(n);
+    for (uint32_t i = 0; i < n; ++i) cbase_h[i] = spec[i].cbase;
+    const uint64_t* cbase_d = upload(cbase_h);
+    uint32_t* fib_first = ar.alloc<uint32_t>(n + 1);
+    launch_key_bounds(fib.key, fib.n, cbase_d, n, fib_first, st);
     CuckooBuildInfo cinfo;
     const CuckooTable table = cuckoo_build(fib.key, fib.n, opt.hash_seed, kn.max_chain, kn.max_load, kn.max_attempts, ar, &cinfo);
     stats.hash_attempts = cinfo.attempts;
@@ -1385,6 +1522,11 @@ Front front_batch(const std::vector<BatchItemHost>& items, uint32_t location, co
     F.nitems = n;
     F.row_first = row_first;
     F.colbase = h_col_first;
+    F.b_off = b_off_d;
+    F.col_first = col_first;
+    F.fib_first = fib_first;
+    F.col_run = cols.run_start;
+    F.ncols_global = cols.nruns;
     stats.ncols = cols.nruns;
     return F;
 }
@@ -1838,17 +1980,21 @@ const char* ptc_last_error(void) {
 ptc_status ptc_contract(const ptc_coo* A, const ptc_coo* B, uint32_t c, const uint32_t* a_modes,
                         const uint32_t* b_modes, const ptc_options* opt, ptc_tensor* out, ptc_stats* stats) {
     ptc::DeviceGuard keep_device;
+    if (out) std::memset(out, 0, sizeof(*out));  // so that every error path below can release it
     try {
         ptc::contract_impl(A, B, c, a_modes, b_modes, opt, out, stats);
         ptc::g_last_error.clear();
         return PTC_OK;
     } catch (const Error& e) {
+        ptc_tensor_free(out);
         ptc::set_last_error(e.status, e.msg);
         return e.status;
     } catch (const std::bad_alloc&) {
+        ptc_tensor_free(out);
         ptc::set_last_error(PTC_ERR_OUT_OF_MEMORY, "host allocation failed");
         return PTC_ERR_OUT_OF_MEMORY;
     } catch (...) {
+        ptc_tensor_free(out);
         ptc::set_last_error(PTC_ERR_INTERNAL, "unexpected exception");
         return PTC_ERR_INTERNAL;
     }

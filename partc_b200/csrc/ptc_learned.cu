@@ -19,32 +19,39 @@ __device__ __forceinline__ float popularity_at(const float* __restrict__ row, fl
 // cnt[i * P + p] = ceil(margin * D_pred(i) * G_p(F_i) / G(F_i)), at most the panel's width and
 // the row's products; D_pred = 2^pred - 1 clamped to [1, min(F, ncols)].  In a batch
 // (row_item != null) a row's columns are its item's: panels past the item's item_cols[item]
-// columns get nothing and the shares are taken over the item's panels (cum = the table's prefix
-// sums over panels).
+// columns get nothing and the shares are taken over the item's panels -- by its own B nonzeros
+// per panel when per-item statistics are given (is.pmass), else by the batch's popularity table
+// (cum = the table's prefix sums over panels).
 __global__ void predicted_panel_counts_kernel(const uint32_t* __restrict__ rows, uint64_t n,
                                               const uint64_t* __restrict__ row_flops, const float* __restrict__ pred,
                                               const float* __restrict__ gp, const float* __restrict__ cum,
                                               const uint32_t* __restrict__ row_item,
                                               const uint32_t* __restrict__ item_cols,
                                               const uint64_t* __restrict__ pbase, uint32_t P, uint32_t panel_log2,
-                                              uint64_t ncols, float margin, uint32_t* __restrict__ cnt) {
+                                              uint64_t ncols, float margin, uint32_t* __restrict__ cnt, ItemStats is) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float F = (float)row_flops[rows[i]];
-    const uint64_t nc = row_item ? item_cols[row_item[rows[i]]] : ncols;
+    const uint32_t item = row_item ? row_item[rows[i]] : 0u;
+    const uint64_t nc = row_item ? item_cols[item] : ncols;
     const uint64_t base = pbase ? pbase[i] : i * P;
     const uint32_t Pi = pbase ? (uint32_t)(pbase[i + 1] - pbase[i]) : P;
     float d = exp2f(pred[i]) - 1.f;
     d = fminf(fmaxf(d, 1.f), fminf(F, (float)nc));
-    const float tot = row_item ? popularity_at(cum + (uint64_t)Pi * kGridPoints, F)
-                               : popularity_at(gp + (uint64_t)P * kGridPoints, F);
+    const bool by_mass = row_item && is.pmass;
+    const float nb_item = by_mass ? (float)(is.b_off[item + 1] - is.b_off[item]) : 0.f;
+    const float tot = by_mass ? 0.f
+                      : row_item ? popularity_at(cum + (uint64_t)Pi * kGridPoints, F)
+                                 : popularity_at(gp + (uint64_t)P * kGridPoints, F);
     for (uint32_t p = 0; p < Pi; ++p) {
         const uint64_t lo = (uint64_t)p << panel_log2;
         if (lo >= nc) {
             cnt[base + p] = 0;
             continue;
         }
-        const float share = tot > 0.f ? popularity_at(gp + (uint64_t)p * kGridPoints, F) / tot : 1.f / Pi;
+        float share;
+        if (by_mass) share = nb_item > 0.f ? (float)is.pmass[is.item_pb[item] + p] / nb_item : 1.f / Pi;
+        else share = tot > 0.f ? popularity_at(gp + (uint64_t)p * kGridPoints, F) / tot : 1.f / Pi;
         const uint64_t width = (nc - lo) < (1ull << panel_log2) ? (nc - lo) : (1ull << panel_log2);
         float c = ceilf(margin * d * share);
         c = fminf(fminf(c, (float)width), F);
@@ -66,18 +73,19 @@ __global__ void popularity_prefix_kernel(const float* __restrict__ gp, uint32_t 
 void launch_predicted_panel_counts(const uint32_t* rows, uint64_t n, const uint64_t* row_flops, const float* pred,
                                    const float* gp, const uint32_t* row_item, const uint32_t* item_cols,
                                    const uint64_t* pbase, uint32_t P, uint32_t panel_log2, uint64_t ncols, float margin,
-                                   uint32_t* cnt, Arena& ar) {
+                                   uint32_t* cnt, Arena& ar, const ItemStats* is) {
     if (n == 0) return;
     cudaStream_t st = ar.stream();
     float* cum = nullptr;
-    if (row_item) {
+    if (row_item && !(is && is->pmass)) {
         cum = ar.alloc<float>((uint64_t)(P + 1) * kGridPoints);
         popularity_prefix_kernel<<<ceil_div_u32(kGridPoints, 128), 128, 0, st>>>(gp, P, cum);
         count_launch();
         PTC_CHECK_LAUNCH();
     }
     predicted_panel_counts_kernel<<<ceil_div_u32(n, 128), 128, 0, st>>>(
-        rows, n, row_flops, pred, gp, cum, row_item, item_cols, pbase, P, panel_log2, ncols, margin, cnt);
+        rows, n, row_flops, pred, gp, cum, row_item, item_cols, pbase, P, panel_log2, ncols, margin, cnt,
+        is ? *is : ItemStats{});
     count_launch();
     PTC_CHECK_LAUNCH();
 }

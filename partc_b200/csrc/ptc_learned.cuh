@@ -7,11 +7,11 @@
 namespace ptc {
 
 // Per-panel predicted counts of the large rows (batches: row_item/item_cols give each row's item
-// and that item's column count; null for a single contraction).
+// and that item's column count, `is` its own panel shares; null for a single contraction).
 void launch_predicted_panel_counts(const uint32_t* rows, uint64_t n, const uint64_t* row_flops, const float* pred,
                                    const float* gp, const uint32_t* row_item, const uint32_t* item_cols,
                                    const uint64_t* pbase, uint32_t P, uint32_t panel_log2, uint64_t ncols, float margin,
-                                   uint32_t* cnt, Arena& ar);
+                                   uint32_t* cnt, Arena& ar, const ItemStats* is = nullptr);
 // *out = sum of x[0..n)
 void launch_sum_u32(const uint32_t* x, uint64_t n, uint64_t* out, cudaStream_t st);
 void launch_gather_parts(const PartItem* parts, const uint32_t* idx, uint32_t n, PartItem* out, cudaStream_t st);

@@ -45,9 +45,28 @@ constexpr int kGridPoints = 41 * kGridPerOctave;
 // gp[p * kGridPoints + g] = G restricted to the columns of panel p (device, npanels * kGridPoints)
 void launch_popularity_table(const uint32_t* b_col, uint64_t nb, uint64_t ncols, uint32_t npanels, uint32_t panel_log2,
                              float* gp, Arena& ar);
-// Per-row features of `rows` (device): x[i * kSizerInputs + f]
+// Per-item statistics of a batch (device arrays indexed by item).  With them every row of a batch
+// gets the features a single contraction of its own item would give it: its item's column,
+// nonzero, fiber and row counts and its item's column popularity, not the whole batch's.
+struct ItemStats {
+    uint32_t nitems = 0;
+    const uint64_t* b_off = nullptr;      // [nitems + 1] first B nonzero of each item
+    const uint32_t* col_first = nullptr;  // [nitems + 1] first (global) column of each item
+    const uint32_t* fib_first = nullptr;  // [nitems + 1] first fiber of each item
+    const uint32_t* row_first = nullptr;  // [nitems + 1] first row of each item
+    const uint32_t* col_run = nullptr;    // [ncols + 1] B nonzeros before each global column (degrees)
+    float* gtot = nullptr;                // [nitems * kGridPoints] each item's G(F) table
+    uint32_t* pmass = nullptr;            // [item_pb[i] + p] B nonzeros in local panel p of item i
+    const uint64_t* item_pb = nullptr;    // [nitems + 1] first panel of each item in pmass
+};
+
+// Fill is.gtot and is.pmass (panels of 2^panel_log2 columns); is.item_pb must be set.
+void launch_item_popularity(ItemStats& is, uint64_t ncols_global, uint32_t panel_log2, Arena& ar);
+
+// Per-row features of `rows` (device): x[i * kSizerInputs + f].  `is` (batches) gives each row
+// its item's statistics; null for a single contraction.
 void launch_row_features(const Operands& op, const uint32_t* rows, uint64_t n, const uint64_t* row_flops,
-                         const float* gp, float* x, cudaStream_t st);
+                         const float* gp, float* x, cudaStream_t st, const ItemStats* is = nullptr);
 // t[i] = log2(1 + row_d[rows[i]])
 void launch_row_targets(const uint32_t* rows, uint64_t n, const uint64_t* row_d, float* t, cudaStream_t st);
 

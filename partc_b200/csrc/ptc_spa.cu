@@ -11,6 +11,8 @@
 //   * products of different A nonzeros that meet in one column are applied in stream order --
 //     by rank inside a warp (match_any), or by claim rounds inside a block.
 // Products use __dmul_rn and sums __dadd_rn so nothing is contracted into an FMA.
+#include <algorithm>
+
 #include "ptc_spa.cuh"
 
 namespace ptc {
@@ -192,27 +194,31 @@ void launch_small_rows(bool numeric, const Operands& op, const uint32_t* rows, u
 }
 
 // ---------------------------------------------------------------------------------------------
-// exact symbolic pass for the other rows: one block per row, a bitmap over every column in
-// shared memory; the first set of a bit is a new output entry, counted per fine panel
+// exact symbolic pass for the other rows: one block per row, a bitmap over the columns in shared
+// memory; the first set of a bit is a new output entry, counted per fine panel.  When the columns
+// do not fit one bitmap, the row is swept in windows of whole panels (each window reads only the
+// fiber entries inside it), so the column count has no limit.
 // ---------------------------------------------------------------------------------------------
 
 constexpr int kSymThreads = 512;
 constexpr int kSymItems = 4;
+constexpr size_t kSymSmemBytes = 200 * 1024;  // bitmap + panel counters of one window
 
 __global__ void __launch_bounds__(kSymThreads)
     sym_bitmap_kernel(Operands op, const uint32_t* __restrict__ rows, uint32_t nrows, uint32_t* __restrict__ panel_cnt,
                       const uint64_t* __restrict__ pbase, uint64_t* __restrict__ row_d,
-                      uint32_t* __restrict__ work_counter, uint32_t nwords) {
+                      uint32_t* __restrict__ work_counter, uint32_t wpanels) {
     extern __shared__ __align__(16) unsigned char smem[];
-    uint32_t* bits = reinterpret_cast<uint32_t*>(smem);   // [nwords]
-    uint32_t* pc = bits + nwords;                         // [npanels]
+    const uint32_t nwords = (uint32_t)((((uint64_t)wpanels << op.panel_log2) + 31) / 32);
+    uint32_t* bits = reinterpret_cast<uint32_t*>(smem);   // [nwords]: the window's columns
+    uint32_t* pc = bits + nwords;                         // [wpanels]: the window's panels
     __shared__ uint32_t ws[kSymThreads], wl[kSymThreads], wscan[kSymThreads];
     __shared__ uint32_t tmp[kSymThreads / 32 + 1];
     __shared__ uint32_t s_item;
     const uint32_t t = threadIdx.x;
     const uint32_t P = op.npanels;
     for (uint32_t i = t; i < nwords; i += kSymThreads) bits[i] = 0;
-    for (uint32_t i = t; i < P; i += kSymThreads) pc[i] = 0;
+    for (uint32_t i = t; i < wpanels; i += kSymThreads) pc[i] = 0;
 
     for (;;) {
         __syncthreads();
@@ -222,75 +228,93 @@ __global__ void __launch_bounds__(kSymThreads)
         if (item >= nrows) break;
         const uint32_t row = rows[item];
         const uint32_t ka = op.row_start[row], kb = op.row_start[row + 1];
-        for (uint32_t kw = ka; kw < kb; kw += kSymThreads) {
-            const uint32_t k = kw + t;
-            uint32_t L = 0, s = 0;
-            if (k < kb) {
-                const int32_t f = op.a_fib[k];
-                if (f >= 0) {
-                    s = op.fib_start[f];
-                    L = op.fib_start[f + 1] - s;
-                }
-            }
-            uint32_t total;
-            const uint32_t excl = block_exclusive_scan<uint32_t, kSymThreads>(L, tmp, &total);
-            ws[t] = s;
-            wl[t] = L;
-            wscan[t] = excl;
-            __syncthreads();
-            for (uint32_t c0 = 0; c0 < total; c0 += kSymThreads * kSymItems) {
-                // blocked: thread t takes products [c0 + t*kSymItems, ... + kSymItems)
-                const uint32_t q0 = c0 + t * kSymItems;
-                uint32_t kk = 0;
-                if (q0 < total) {
-                    uint32_t hi = kSymThreads;
-                    while (hi - kk > 1) {
-                        const uint32_t mid = (kk + hi) >> 1;
-                        if (wscan[mid] <= q0) kk = mid; else hi = mid;
-                    }
-                }
-#pragma unroll
-                for (int i = 0; i < kSymItems; ++i) {
-                    const uint32_t q = q0 + i;
-                    uint32_t panel = 0xffffffffu;
-                    if (q < total) {
-                        while (kk + 1 < kSymThreads && wscan[kk] + wl[kk] <= q) ++kk;
-                        const uint32_t col = op.b_col[ws[kk] + (q - wscan[kk])];
-                        const uint32_t bit = 1u << (col & 31);
-                        const uint32_t old = atomicOr(&bits[col >> 5], bit);
-                        if (!(old & bit)) panel = col >> op.panel_log2;
-                    }
-                    const uint32_t m = __match_any_sync(kFullMask, panel);
-                    if (panel != 0xffffffffu && (m & lanemask_lt()) == 0) atomicAdd(&pc[panel], (uint32_t)__popc(m));
-                }
-            }
-            __syncthreads();
-        }
-        uint32_t dsum = 0;
         const uint64_t pb = pbase ? pbase[item] : (uint64_t)item * P;
         const uint32_t pn = pbase ? (uint32_t)(pbase[item + 1] - pbase[item]) : P;  // the row's item's panels
-        // a row's columns lie in its item's panels: only those counters and bitmap words were set
-        for (uint32_t p = t; p < pn; p += kSymThreads) {
-            const uint32_t v = pc[p];
-            panel_cnt[pb + p] = v;
-            dsum += v;
-            pc[p] = 0;
+        uint32_t dsum = 0;
+        // a row's columns lie in its item's panels: only those counters and bitmap words are set
+        for (uint32_t wp0 = 0; wp0 < pn; wp0 += wpanels) {
+            const uint32_t wp1 = min(pn, wp0 + wpanels);
+            const bool whole = wp0 == 0 && wp1 == pn;  // one window: every fiber entry is inside it
+            const uint32_t wc0 = wp0 << op.panel_log2;
+            for (uint32_t kw = ka; kw < kb; kw += kSymThreads) {
+                const uint32_t k = kw + t;
+                uint32_t L = 0, s = 0;
+                if (k < kb) {
+                    const int32_t f = op.a_fib[k];
+                    if (f >= 0) {
+                        uint32_t e;
+                        if (whole) {
+                            s = op.fib_start[f];
+                            e = op.fib_start[f + 1];
+                        } else {
+                            part_range(op, f, wp0, wp1, s, e);
+                        }
+                        L = e - s;
+                    }
+                }
+                uint32_t total;
+                const uint32_t excl = block_exclusive_scan<uint32_t, kSymThreads>(L, tmp, &total);
+                ws[t] = s;
+                wl[t] = L;
+                wscan[t] = excl;
+                __syncthreads();
+                for (uint32_t c0 = 0; c0 < total; c0 += kSymThreads * kSymItems) {
+                    // blocked: thread t takes products [c0 + t*kSymItems, ... + kSymItems)
+                    const uint32_t q0 = c0 + t * kSymItems;
+                    uint32_t kk = 0;
+                    if (q0 < total) {
+                        uint32_t hi = kSymThreads;
+                        while (hi - kk > 1) {
+                            const uint32_t mid = (kk + hi) >> 1;
+                            if (wscan[mid] <= q0) kk = mid; else hi = mid;
+                        }
+                    }
+#pragma unroll
+                    for (int i = 0; i < kSymItems; ++i) {
+                        const uint32_t q = q0 + i;
+                        uint32_t panel = 0xffffffffu;
+                        if (q < total) {
+                            while (kk + 1 < kSymThreads && wscan[kk] + wl[kk] <= q) ++kk;
+                            const uint32_t col = op.b_col[ws[kk] + (q - wscan[kk])] - wc0;
+                            const uint32_t bit = 1u << (col & 31);
+                            const uint32_t old = atomicOr(&bits[col >> 5], bit);
+                            if (!(old & bit)) panel = col >> op.panel_log2;
+                        }
+                        const uint32_t m = __match_any_sync(kFullMask, panel);
+                        if (panel != 0xffffffffu && (m & lanemask_lt()) == 0) atomicAdd(&pc[panel], (uint32_t)__popc(m));
+                    }
+                }
+                __syncthreads();
+            }
+            for (uint32_t p = t; p < wp1 - wp0; p += kSymThreads) {
+                const uint32_t v = pc[p];
+                panel_cnt[pb + wp0 + p] = v;
+                dsum += v;
+                pc[p] = 0;
+            }
+            const uint32_t rw = (uint32_t)((((uint64_t)(wp1 - wp0) << op.panel_log2) + 31) / 32);
+            for (uint32_t i = t; i < rw; i += kSymThreads) bits[i] = 0;
+            __syncthreads();
         }
-        const uint32_t rw = (uint32_t)min((uint64_t)nwords, (((uint64_t)pn << op.panel_log2) + 31) / 32);
-        for (uint32_t i = t; i < rw; i += kSymThreads) bits[i] = 0;
         dsum = warp_sum(dsum);
         if (lane_id() == 0 && dsum) atomicAdd(reinterpret_cast<unsigned long long*>(&row_d[row]), (unsigned long long)dsum);
     }
 }
 
-uint32_t sym_bitmap_max_cols() { return 1536u * 1024u; }  // 192 KiB of bitmap
+// Panels of one window: as many as fit the shared-memory budget (bitmap + counters).
+uint32_t sym_window_panels(uint32_t npanels, uint32_t panel_log2) {
+    const uint64_t per_panel = ((1ull << panel_log2) + 31) / 32 * 4 + 4;  // bitmap words + counter
+    const uint64_t fit = std::max<uint64_t>(1, kSymSmemBytes / per_panel);
+    return (uint32_t)std::min<uint64_t>(npanels, fit);
+}
 
 void launch_sym_bitmap(const Operands& op, const uint32_t* rows, uint32_t nrows, uint32_t* panel_cnt,
                        const uint64_t* pbase, uint64_t* row_d,
                        uint32_t* work_counter, int num_sms, cudaStream_t st) {
     if (nrows == 0) return;
-    const uint32_t nwords = (uint32_t)((op.ncols + 31) / 32);
-    const size_t smem = (size_t)(nwords + op.npanels) * sizeof(uint32_t);
+    const uint32_t wpanels = sym_window_panels(op.npanels, op.panel_log2);
+    const uint32_t nwords = (uint32_t)((((uint64_t)wpanels << op.panel_log2) + 31) / 32);
+    const size_t smem = (size_t)(nwords + wpanels) * sizeof(uint32_t);
     PTC_CUDA(cudaMemsetAsync(work_counter, 0, sizeof(uint32_t), st));
     PTC_CUDA(cudaFuncSetAttribute(sym_bitmap_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 1;
@@ -298,7 +322,7 @@ void launch_sym_bitmap(const Operands& op, const uint32_t* rows, uint32_t nrows,
     per_sm = per_sm < 1 ? 1 : per_sm;
     const uint32_t grid = (uint32_t)std::min<uint64_t>(nrows, (uint64_t)num_sms * per_sm);
     sym_bitmap_kernel<<<grid, kSymThreads, smem, st>>>(op, rows, nrows, panel_cnt, pbase, row_d, work_counter,
-                                                         nwords);
+                                                         wpanels);
     count_launch();
     PTC_CHECK_LAUNCH();
 }

@@ -13,8 +13,6 @@ uint32_t hash_part_capacity();
 uint32_t dense_part_columns();
 // smallest open-addressing table (log2 slots) a part uses
 uint32_t hash_part_min_bits();
-// largest column count the bitmap symbolic pass handles
-uint32_t sym_bitmap_max_cols();
 
 // small rows: symbolic (row_d[row] = output nnz) or numeric (writes at row_off[row])
 void launch_small_rows(bool numeric, const Operands& op, const uint32_t* rows, uint32_t nrows, uint64_t* row_d,

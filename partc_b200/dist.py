@@ -8,7 +8,9 @@ maximum of the ranks' elapsed times (NCCL on GPUs, gloo in the CPU tests).
 from __future__ import annotations
 
 import os
-from typing import Optional
+import socket
+import sys
+from typing import List, Optional
 
 
 def rank_env():
@@ -59,3 +61,23 @@ def job_throughput(units_per_rank_step: float, steps: int, world: int, max_secon
 def runs_reference_arm(rank: int) -> bool:
     """The CPU reference arm runs on rank 0 only; the other ranks exit without work."""
     return rank == 0
+
+
+def needs_launcher(gpus: int) -> bool:
+    """True when N > 1 GPUs were asked for but this process was not started by a launcher."""
+    return gpus > 1 and "WORLD_SIZE" not in os.environ
+
+
+def free_port() -> int:
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def launcher_command(script: str, argv: List[str], gpus: int, port: Optional[int] = None) -> List[str]:
+    """torchrun command that starts `script argv` as `gpus` ranks on this node (one per GPU),
+    rendezvous on 127.0.0.1."""
+    return [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={gpus}",
+            "--master-addr=127.0.0.1", f"--master-port={port or free_port()}", script, *argv]

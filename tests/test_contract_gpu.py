@@ -59,6 +59,20 @@ def test_general_two_tensors(engine, oracle_mod):
     assert_same_output(idx, vals, o["idx"], o["vals"], bit_exact=True)
 
 
+@pytest.mark.parametrize("path", ["two_phase", "learned"])
+def test_more_than_two_million_columns(engine, oracle_mod, path):
+    """B with about 2.6M distinct free keys (columns): more than one shared-memory bitmap holds, so
+    the exact symbolic pass sweeps each row in column windows.  The reference sizes each row's
+    accumulator by the row alone (fksCuckooSPA.hpp:637-645) and has no column limit either."""
+    B = gen.random_coo([4000, 3000, 3000], 3_000_000, [None] * 3, 41, "uniform01")
+    A = gen.random_coo([4000, 50], 2_000, [None, None], 42, "uniform11")
+    o = oracle_mod.contract(A, B, 1, [0, 1], [0, 1, 2])
+    idx, vals, st = engine.contract(A, B, 1, [0, 1], [0, 1, 2], path=path)
+    assert st["ncols"] > 2_000_000
+    assert st["mult_adds"] == o["flops"]
+    assert_same_output(idx, vals, o["idx"], o["vals"], bit_exact=True)
+
+
 def test_output_is_canonical_for_panel_rows(engine, oracle_mod):
     """Rows come out in increasing free-key order; panel rows in increasing column order."""
     t = gen.random_coo([50, 40, 3000], 100_000, [None, None, 1.0], 33, "uniform01")

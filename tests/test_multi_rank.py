@@ -54,3 +54,14 @@ def test_single_process_defaults(monkeypatch):
     assert pdist.max_over_ranks(3.5) == 3.5
     with pytest.raises(ValueError):
         pdist.job_throughput(1, 1, 1, 0.0)
+
+
+def test_launcher_command(monkeypatch):
+    monkeypatch.delenv("WORLD_SIZE", raising=False)
+    assert pdist.needs_launcher(4) and not pdist.needs_launcher(1)
+    monkeypatch.setenv("WORLD_SIZE", "4")
+    assert not pdist.needs_launcher(4)
+    cmd = pdist.launcher_command("bench.py", ["--gpus", "4", "--steps", "2"], 4, port=29511)
+    assert cmd[1:3] == ["-m", "torch.distributed.run"]
+    assert "--nproc-per-node=4" in cmd and "--master-addr=127.0.0.1" in cmd and "--master-port=29511" in cmd
+    assert cmd[-5:] == ["bench.py", "--gpus", "4", "--steps", "2"]
