@@ -113,8 +113,16 @@ typedef struct ptc_options {
                                        failures, twice the buckets (the reference's rehash with new
                                        kDict pairs and a larger table, fksCuckoo.hpp:297-442), before
                                        the call returns PTC_ERR_HASH_BUILD (default 8) */
-    uint32_t reserved[2];
+    uint32_t large_rows;            /* accumulator of the large rows of a single contraction:
+                                       PTC_LARGE_ROWS_AUTO (0, default: the row bitmap when the
+                                       columns fit it), PTC_LARGE_ROWS_BITMAP (one block per row,
+                                       a bitmap of its columns in shared memory, up to about 600k
+                                       distinct B free keys) or PTC_LARGE_ROWS_PANELS (warp tasks
+                                       and block parts over column panels, any size) */
+    uint32_t reserved[1];
 } ptc_options;
+
+enum { PTC_LARGE_ROWS_AUTO = 0, PTC_LARGE_ROWS_BITMAP = 1, PTC_LARGE_ROWS_PANELS = 2 };
 
 /* Per-call statistics; every time is measured with CUDA events on the call's stream. */
 typedef struct ptc_stats {
@@ -239,7 +247,8 @@ typedef struct ptc_tune_report {
 
 /*
  * Autotuner (no counterpart in the reference): picks the tuning knobs of ptc_options --
- * panel_width (shared-table column ranges), small_max_products / warp_task_max_len /
+ * large_rows (row bitmap or panel kernels), panel_width (shared-table column ranges),
+ * small_max_products / warp_task_max_len /
  * sort_max_avg_products (which accumulator, and so how many threads, each row gets) and
  * hash_load_pct (cuckoo table load factor) -- for the given items by timing
  * ptc_batch_contract on them (outputs discarded) under candidate settings, one knob at a time from

@@ -62,7 +62,7 @@ class Options(C.Structure):
                 ("sort_rows", C.c_uint32), ("small_max_products", C.c_uint32),
                 ("sort_max_avg_products", C.c_uint32), ("hash_load_pct", C.c_uint32),
                 ("batch_wave_mib", C.c_uint32), ("warp_task_max_len", C.c_uint32), ("cuckoo_max_chain", C.c_uint32),
-                ("cuckoo_max_attempts", C.c_uint32), ("reserved", C.c_uint32 * 2)]
+                ("cuckoo_max_attempts", C.c_uint32), ("large_rows", C.c_uint32), ("reserved", C.c_uint32 * 1)]
 
 
 class Stats(C.Structure):
@@ -93,7 +93,8 @@ class TuneReport(C.Structure):
     _fields_ = [("trials", C.c_uint32), ("repeats", C.c_uint32), ("default_ms", C.c_double),
                 ("best_ms", C.c_double), ("reserved", C.c_double * 4)]
 
-TUNE_KNOBS = ("panel_width", "warp_task_max_len", "small_max_products", "sort_max_avg_products", "hash_load_pct")
+TUNE_KNOBS = ("large_rows", "panel_width", "warp_task_max_len", "small_max_products", "sort_max_avg_products",
+              "hash_load_pct")
 
 
 class TrainOptions(C.Structure):
@@ -178,6 +179,8 @@ def options(**kw) -> Options:
             v = {"two_phase": PATH_TWO_PHASE, "learned": PATH_LEARNED}[v]
         if k == "output_location" and isinstance(v, str):
             v = {"host": PTC_HOST, "device": PTC_DEVICE}[v]
+        if k == "large_rows" and isinstance(v, str):
+            v = {"auto": 0, "bitmap": 1, "panels": 2}[v]
         setattr(o, k, v)
     return o
 

@@ -28,6 +28,7 @@
 #include "ptc_learned.cuh"
 #include "ptc_sizer.cuh"
 #include "ptc_spa.cuh"
+#include "ptc_rowmap.cuh"
 
 namespace ptc {
 
@@ -508,6 +509,7 @@ ptc_options resolve_options(const ptc_options* opt_in) {
     PTC_REQUIRE(opt.panel_width == 0 || (opt.panel_width >= 32 && opt.panel_width <= 4096 &&
                                          (opt.panel_width & (opt.panel_width - 1)) == 0),
                 PTC_ERR_INVALID_ARGUMENT, "panel_width must be 0 or a power of two in [32, 4096]");
+    PTC_REQUIRE(opt.large_rows <= PTC_LARGE_ROWS_PANELS, PTC_ERR_INVALID_ARGUMENT, "bad large_rows");
     PTC_REQUIRE(opt.path == PTC_PATH_TWO_PHASE || opt.path == PTC_PATH_LEARNED, PTC_ERR_INVALID_ARGUMENT,
                 "bad path");
     return opt;
@@ -656,6 +658,46 @@ uint64_t learned_reruns(const Operands& op, std::vector<Launched> groups, const 
     return read_scalar(ov.cursor, st) - read_scalar(ov.overshoot, st);
 }
 
+// Learned path on the row bitmap kernel: rows whose claim did not fit the predicted output are
+// listed in mo.fail_list (their exact counts in mo.item_count); the output grows to hold them
+// and they run again, claiming after the entries already written (their sizes are now known, so
+// they cannot fail again).  Returns the output nnz.
+uint64_t rowmap_reruns(const Operands& op, const uint32_t* rows, uint32_t nrows, const float* pred,
+                       const OutputView& mo, OutputView& ov, uint32_t* work_counter, int num_sms, Arena& ar,
+                       ptc_stats& stats) {
+    cudaStream_t st = ar.stream();
+    const uint32_t nfail = read_scalar(mo.fail_count, st);
+    if (nrows > 0) {  // the sizer's error over the rows it sized (every row's exact count is known)
+        uint64_t* row_actual = ar.alloc<uint64_t>(op.nrows);
+        launch_scatter_counts(rows, nrows, mo.item_count, row_actual, st);
+        double* esum = ar.alloc<double>(1);
+        launch_log2_error(rows, nrows, pred, row_actual, esum, st);
+        stats.sizer_mean_abs_log2_err = read_scalar(esum, st) / nrows;
+    }
+    stats.rerun_rows = nfail;
+    if (nfail > 0) {
+        uint32_t* again = ar.alloc<uint32_t>(nfail);
+        uint32_t* cnt = ar.alloc<uint32_t>(nfail);
+        launch_gather<uint32_t>(rows, mo.fail_list, nfail, again, st);
+        launch_gather<uint32_t>(mo.item_count, mo.fail_list, nfail, cnt, st);
+        uint64_t* need = ar.alloc<uint64_t>(1);
+        launch_sum_u32(cnt, nfail, need, st);
+        const uint64_t used = read_scalar(ov.cursor, st) - read_scalar(ov.overshoot, st);
+        const uint64_t want = used + read_scalar(need, st);
+        if (want > ov.capacity) grow_output(ov, op.fa + op.fb, used, want + 1024, st);
+        PTC_CUDA(cudaMemcpyAsync(ov.cursor, &used, sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+        PTC_CUDA(cudaMemsetAsync(ov.overshoot, 0, sizeof(uint64_t), st));
+        OutputView o2 = ov;
+        o2.fail_count = mo.fail_count;
+        o2.fail_list = ar.alloc<uint32_t>(nfail);
+        o2.item_count = nullptr;
+        PTC_CUDA(cudaMemsetAsync(o2.fail_count, 0, sizeof(uint32_t), st));
+        launch_rowmap(kRowmapClaim, op, again, nfail, nullptr, nullptr, o2, work_counter, num_sms, st);
+        PTC_REQUIRE(read_scalar(o2.fail_count, st) == 0, PTC_ERR_INTERNAL, "exactly sized rows failed again");
+    }
+    return read_scalar(ov.cursor, st) - read_scalar(ov.overshoot, st);
+}
+
 // Training samples of the learned sizer, gathered instead of running the numeric pass.
 struct Collect {
     std::vector<float> x;  // n * kSizerInputs
@@ -738,6 +780,11 @@ struct Plan {
     uint64_t* copy_keys = nullptr;   // the same row ids as sort keys (wave slices)
     uint32_t n_copy = 0;
     bool collected = false;
+    // large rows of a single contraction on the row bitmap kernel (instead of parts): the rows
+    // it writes, heaviest first (the two-phase path leaves the collision-free rows to copy_rows)
+    bool rowmap = false;
+    uint32_t* map_rows = nullptr;
+    uint32_t n_map = 0;
 };
 
 // One kind of work item and its accumulator kernel.
@@ -808,7 +855,13 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
     const uint32_t n_small = pl.n_small, n_big = pl.n_big, n_esc = pl.n_esc;
     // large rows: warp tasks for rows of at most kWarpTaskMaxLen A nonzeros (panels of at most
     // a dense warp task's width), block parts for the others; each group largest first
-    const uint32_t warp_len = (opt.panel_width == 0 || opt.panel_width <= warp_task_dense_columns())
+    // the row bitmap kernel takes every large row of a single contraction whose columns fit it
+    // (a batch's columns are its items' own: the widest item decides)
+    pl.rowmap = opt.large_rows != PTC_LARGE_ROWS_PANELS && ncols <= rowmap_max_cols();
+    PTC_REQUIRE(!(opt.large_rows == PTC_LARGE_ROWS_BITMAP && !pl.rowmap), PTC_ERR_INVALID_ARGUMENT,
+                "large_rows = PTC_LARGE_ROWS_BITMAP: at most about 600k distinct B free keys per contraction");
+    const uint32_t warp_len = pl.rowmap ? UINT32_MAX
+                              : (opt.panel_width == 0 || opt.panel_width <= warp_task_dense_columns())
                                   ? (opt.warp_task_max_len ? opt.warp_task_max_len : kWarpTaskMaxLen) : 0u;
     if (n_big > 0) {
         uint64_t* wkey = ar.alloc<uint64_t>(n_big);
@@ -844,19 +897,24 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
             e += (uint64_t)(F.h_row_first[i + 1] - F.h_row_first[i]) * std::max<uint64_t>(1, (item_cols_h[i] + w - 1) / w);
         return e;
     };
-    if (W == 0) {  // at most 256 columns (a third of a dense warp task), wider for small tables
+    if (pl.rowmap) {
+        // the row bitmap kernel needs no panels: one panel spans every column (the sizer's
+        // popularity table then has a single panel)
+        W = 1;
+        while ((uint64_t)W < ncols) W <<= 1;
+    } else if (W == 0) {  // at most 256 columns (a third of a dense warp task), wider for small tables
         W = 32;
         while (W < 256 && (uint64_t)W * 16 < ncols) W <<= 1;
         // wider panels for big tables, but never wider than a dense warp task (a single panel
         // above a sparse task's capacity becomes a dense task over that panel)
         while (2 * W <= warp_task_dense_columns() && panel_entries(W) * 4 > (2ull << 30)) W <<= 1;
     }
-    PTC_REQUIRE(W <= hash_part_capacity(), PTC_ERR_INVALID_ARGUMENT, "panel_width larger than a hash part");
+    PTC_REQUIRE(pl.rowmap || W <= hash_part_capacity(), PTC_ERR_INVALID_ARGUMENT, "panel_width larger than a hash part");
     pl.W = W;
     pl.log2w = floor_log2(W);
     pl.P = (uint32_t)std::max<uint64_t>(1, (ncols + W - 1) / W);
     const uint32_t P = pl.P;
-    stats.panel_width = W;
+    stats.panel_width = pl.rowmap ? 0 : W;
     uint32_t* panel_off = nullptr;
     if (P > 1 && table_bytes(W) <= kPanelTableBytes) {
         panel_off = ar.alloc<uint32_t>(nfib * (uint64_t)(P + 1));
@@ -901,6 +959,7 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
         uint32_t* ic = ar.alloc<uint32_t>(F.nitems);
         PTC_CUDA(cudaMemcpyAsync(ic, item_cols_h.data(), F.nitems * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
         item_cols = ic;
+        op.item_cols = ic;
         uint64_t* pb = ar.alloc<uint64_t>((uint64_t)n_big + 1);
         launch_row_panel_counts(pl.big_rows, n_big, op.row_item, item_cols, pl.log2w, pb, st);
         exclusive_scan<uint64_t>(pb, pb, n_big, ar);
@@ -911,8 +970,11 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
     pl.work_counter = ar.alloc<uint32_t>(1);
     OutputView none;
     launch_small_rows(false, op, pl.small_rows, n_small, row_d, nullptr, none, st);
-    if (!pl.learned)
-        launch_sym_bitmap(op, pl.big_rows, n_big, panel_cnt, pbase, row_d, pl.work_counter, num_sms, st);
+    if (!pl.learned) {
+        if (pl.rowmap) launch_rowmap(kRowmapCount, op, pl.big_rows, n_big, row_d, nullptr, none, pl.work_counter,
+                                     num_sms, st);
+        else launch_sym_bitmap(op, pl.big_rows, n_big, panel_cnt, pbase, row_d, pl.work_counter, num_sms, st);
+    }
     // sort-based rows: expand their products in stream order, sort stably by (row, column)
     pl.esc_colbits = (uint32_t)colbits;
     if (n_esc > 0) {
@@ -1020,6 +1082,26 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
             launch_row_keys(pl.copy_rows, pl.n_copy, pl.copy_keys, st);
             radix_sort_pairs(pl.copy_keys, pl.copy_rows, pl.n_copy, 0, bits_for_space(nrows), ar);
         }
+    }
+
+    if (pl.rowmap) {
+        // the rows the bitmap kernel writes: every large row but the collision-free ones, in
+        // big_rows' heaviest-first order
+        pl.map_rows = pl.big_rows;
+        pl.n_map = n_big;
+        if (skip_off && n_big > 0 && pl.n_copy > 0) {
+            uint32_t* flag = ar.alloc<uint32_t>((uint64_t)n_big + 1);
+            uint32_t* pos = ar.alloc<uint32_t>((uint64_t)n_big + 1);
+            launch_table_row_flags(pl.big_rows, n_big, skip_off, skip_flops, flag, st);
+            exclusive_scan<uint32_t>(flag, pos, n_big, ar);
+            pl.n_map = read_scalar(pos + n_big, st);
+            uint32_t* sel = ar.alloc<uint32_t>(std::max<uint32_t>(pl.n_map, 1));
+            launch_compact_indices(flag, pos, n_big, sel, st);
+            pl.map_rows = ar.alloc<uint32_t>(std::max<uint32_t>(pl.n_map, 1));
+            launch_gather<uint32_t>(pl.big_rows, sel, pl.n_map, pl.map_rows, st);
+        }
+        stats.hash_parts = 0;
+        return pl;
     }
 
     // split large rows into tasks / parts that fit a shared-memory table
@@ -1191,7 +1273,19 @@ void contract_impl(const ptc_coo* A, const ptc_coo* Bin, uint32_t c, const uint3
         std::vector<Launched> groups;
         launch_small_rows(true, op, pl.small_rows, pl.n_small, nullptr, pl.row_off, ov, st);
         launch_copy_rows(op, pl.copy_rows, pl.n_copy, pl.alen, pl.row_off, ov, dev.num_sms, st);
-        for (int kind = 0; kind < 2; ++kind) {
+        OutputView mo = ov;  // the row bitmap kernel's view (claim bookkeeping on the learned path)
+        if (pl.rowmap) {
+            if (learned) {
+                const uint32_t n = std::max<uint32_t>(pl.n_map, 1);
+                mo.fail_count = ar.alloc<uint32_t>(1);
+                mo.fail_list = ar.alloc<uint32_t>(n);
+                mo.item_count = ar.alloc<uint32_t>(n);
+                PTC_CUDA(cudaMemsetAsync(mo.fail_count, 0, sizeof(uint32_t), st));
+            }
+            launch_rowmap(learned ? kRowmapClaim : kRowmapExact, op, pl.map_rows, pl.n_map, nullptr, pl.row_off, mo,
+                          pl.work_counter, dev.num_sms, st);
+        }
+        for (int kind = 0; kind < 2 && !pl.rowmap; ++kind) {
             OutputView o = ov;
             if (learned) {
                 const uint32_t n = std::max<uint32_t>(pl.n_parts[kind], 1);
@@ -1205,7 +1299,10 @@ void contract_impl(const ptc_coo* A, const ptc_coo* Bin, uint32_t c, const uint3
         }
         launch_esc_fold(op, ov, pl.esc_run_key, pl.esc_run_start, 0, pl.esc_runs, pl.esc_colbits, pl.esc_rows,
                         pl.esc_first, pl.row_off, pl.esc_sorted, st);
-        if (learned) {
+        if (learned && pl.rowmap) {
+            out_nnz = rowmap_reruns(op, pl.map_rows, pl.n_map, pl.pred, mo, ov, pl.work_counter, dev.num_sms, ar,
+                                    stats);
+        } else if (learned) {
             out_nnz = learned_reruns(op, groups, pl.big_rows, pl.n_big, pl.pred, pl.rule[1], ov, pl.work_counter,
                                      op.err, dev.num_sms, op.nrows, ar, stats);
         }
@@ -1661,6 +1758,29 @@ void batch_impl(const std::vector<BatchItemHost>& items, uint32_t location, cons
         PTC_CUDA(cudaMemcpyAsync(pb[kind].data(), bounds, (nw + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         PTC_CUDA(cudaStreamSynchronize(st));
     }
+    // rows of the bitmap kernel by wave (heaviest first inside a wave: the sort is stable)
+    const uint32_t* map_rows = pl.map_rows;
+    std::vector<uint32_t> mb(nw + 1, 0);
+    mb[nw] = pl.n_map;
+    if (pl.rowmap && nw > 1 && pl.n_map > 0) {
+        uint64_t* key = ar.alloc<uint64_t>(pl.n_map);
+        uint32_t* idx = ar.alloc<uint32_t>(pl.n_map);
+        launch_row_wave(pl.map_rows, pl.n_map, wave_row_d, nw, key, idx, st);
+        radix_sort_pairs(key, idx, pl.n_map, 0, bits_for_space(nw), ar);
+        uint32_t* sorted = ar.alloc<uint32_t>(pl.n_map);
+        launch_gather<uint32_t>(pl.map_rows, idx, pl.n_map, sorted, st);
+        map_rows = sorted;
+        uint32_t* bounds = ar.alloc<uint32_t>(nw + 1);
+        launch_key_bounds(key, pl.n_map, wid_d, nw, bounds, st);
+        PTC_CUDA(cudaMemcpyAsync(mb.data(), bounds, (nw + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        PTC_CUDA(cudaStreamSynchronize(st));
+    }
+    uint32_t* map_fail_count = nullptr;
+    uint32_t* map_fail_list = nullptr;
+    if (learned && pl.rowmap) {
+        map_fail_count = ar.alloc<uint32_t>(1);
+        map_fail_list = ar.alloc<uint32_t>(std::max<uint32_t>(pl.n_map, 1));
+    }
     const std::vector<uint32_t> sb = read_at<uint32_t>(pl.small_pos, wave_row, ar);
     std::vector<uint32_t> cb(nw + 1, 0);  // collision-free rows of each wave (sorted by row)
     if (pl.n_copy > 0) {
@@ -1761,15 +1881,22 @@ void batch_impl(const std::vector<BatchItemHost>& items, uint32_t location, cons
             ov.idx = blk_idx;
             ov.val = blk_val;
             OutputView ovk[2] = {ov, ov};
-            if (learned)
+            OutputView ovm = ov;
+            if (learned) {
                 for (int kind = 0; kind < 2; ++kind) {
                     ovk[kind].fail_count = fail_count[kind];
                     ovk[kind].fail_list = fail_list[kind];
                     PTC_CUDA(cudaMemsetAsync(fail_count[kind], 0, sizeof(uint32_t), st));
                 }
+                if (pl.rowmap) {
+                    ovm.fail_count = map_fail_count;
+                    ovm.fail_list = map_fail_list;
+                    PTC_CUDA(cudaMemsetAsync(map_fail_count, 0, sizeof(uint32_t), st));
+                }
+            }
             PTC_CUDA(cudaEventRecord(ev.ev[EV_WAVE0], st));
             const bool work = sb[w + 1] > sb[w] || pb[0][w + 1] > pb[0][w] || pb[1][w + 1] > pb[1][w] ||
-                              rb[w + 1] > rb[w] || cb[w + 1] > cb[w];
+                              rb[w + 1] > rb[w] || cb[w + 1] > cb[w] || mb[w + 1] > mb[w];
             // the wave's numeric pass, captured and launched as one graph
             cudaGraph_t graph = nullptr;
             cudaGraphExec_t exec = nullptr;
@@ -1783,6 +1910,9 @@ void batch_impl(const std::vector<BatchItemHost>& items, uint32_t location, cons
                     for (int kind = 0; kind < 2; ++kind)
                         launch_parts(kind, op, parts[kind] + pb[kind][w], pb[kind][w + 1] - pb[kind][w], ovk[kind],
                                      pl.work_counter, op.err, dev.num_sms, st);
+                    if (pl.rowmap)
+                        launch_rowmap(learned ? kRowmapClaim : kRowmapExact, op, map_rows + mb[w], mb[w + 1] - mb[w],
+                                      nullptr, pl.row_off, ovm, pl.work_counter, dev.num_sms, st);
                     launch_esc_fold(op, ov, pl.esc_run_key, pl.esc_run_start, rb[w], rb[w + 1], pl.esc_colbits,
                                     pl.esc_rows, pl.esc_first, pl.row_off, pl.esc_sorted, st);
                 } catch (...) {
@@ -1824,6 +1954,18 @@ void batch_impl(const std::vector<BatchItemHost>& items, uint32_t location, cons
                                 (uint32_t)(std::upper_bound(rf.begin(), rf.end(), p.row) - rf.begin()) - 1;
                             failed[it] = 1;
                         }
+                    }
+                }
+                if (pl.rowmap) {  // rows whose claim did not fit their item's budget
+                    const uint32_t nfail = read_scalar(map_fail_count, st);
+                    if (nfail > 0) {
+                        uint32_t* fr = ar.alloc<uint32_t>(nfail);
+                        launch_gather<uint32_t>(map_rows + mb[w], map_fail_list, nfail, fr, st);
+                        std::vector<uint32_t> hr(nfail);
+                        PTC_CUDA(cudaMemcpyAsync(hr.data(), fr, nfail * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+                        PTC_CUDA(cudaStreamSynchronize(st));
+                        for (uint32_t r : hr)
+                            failed[(uint32_t)(std::upper_bound(rf.begin(), rf.end(), r) - rf.begin()) - 1] = 1;
                     }
                 }
                 std::vector<uint64_t> cur(i1 - i0), over(i1 - i0);
@@ -2131,6 +2273,9 @@ std::vector<BatchItemHost> batch_host_items(const ptc_batch_item* items, uint32_
 }
 
 // Median time (ms, the calls' own event clocks) of `repeats` discarded-output runs.
+// Median time of `repeats` runs of the items under `opt`: one item runs as the single
+// contraction it is (ptc_contract's kernels, output kept on the device and released), more as a
+// batch (outputs discarded).
 double time_batch(const std::vector<BatchItemHost>& hi, uint32_t location, const ptc_options& opt, uint32_t repeats) {
     BatchTarget tg;
     tg.ids.resize(hi.size());
@@ -2139,7 +2284,17 @@ double time_batch(const std::vector<BatchItemHost>& hi, uint32_t location, const
     for (uint32_t r = 0; r < repeats; ++r) {
         ptc_stats st;
         std::memset(&st, 0, sizeof(st));
-        batch_chunks(hi, location, opt, tg, st);
+        if (hi.size() == 1) {
+            const BatchItemHost& x = hi[0];
+            ptc_options o = opt;
+            o.output_location = PTC_DEVICE;
+            o.verbose = 0;
+            ptc_tensor out;
+            contract_impl(x.A, x.self ? nullptr : x.B, x.c, x.a_modes, x.b_modes, &o, &out, &st);
+            ptc_tensor_free(&out);
+        } else {
+            batch_chunks(hi, location, opt, tg, st);
+        }
         t.push_back(st.t_total_ms);
     }
     std::sort(t.begin(), t.end());
@@ -2174,6 +2329,7 @@ ptc_status ptc_autotune(const ptc_batch_item* items, uint32_t n, const ptc_optio
             std::vector<uint32_t> values;
         };
         const std::vector<Knob> knobs = {
+            {&ptc_options::large_rows, {PTC_LARGE_ROWS_AUTO, PTC_LARGE_ROWS_PANELS}},
             {&ptc_options::panel_width, {0, 64, 128, 256, 512, 1024}},
             {&ptc_options::warp_task_max_len, {0, 256, 4096, 16384}},
             {&ptc_options::small_max_products, {0, 64, 256, 512}},
@@ -2183,6 +2339,9 @@ ptc_status ptc_autotune(const ptc_batch_item* items, uint32_t n, const ptc_optio
         const uint32_t user_panel = opt.panel_width;
         for (const Knob& k : knobs) {
             if (k.field == &ptc_options::panel_width && user_panel != 0) continue;  // the caller fixed it
+            // panel knobs matter only where the panel kernels run
+            const bool panel_knob = k.field == &ptc_options::panel_width || k.field == &ptc_options::warp_task_max_len;
+            if (panel_knob && n == 1 && opt.large_rows != PTC_LARGE_ROWS_PANELS) continue;
             const uint32_t start = opt.*k.field;
             for (uint32_t v : k.values) {
                 if (v == start) continue;

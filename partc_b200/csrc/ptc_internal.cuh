@@ -51,6 +51,7 @@ struct Operands {
     // is the row's item and item_out[item] says where that item's output and columns start
     const uint32_t* row_item = nullptr;
     const struct ItemOut* item_out = nullptr;
+    const uint32_t* item_cols = nullptr;  // columns of each item (its local column ids are below this)
 };
 
 // One item of a batch inside an output block.  Entry e of the item (e >= ent0, in the batch's entry

@@ -77,8 +77,13 @@ __device__ __forceinline__ bool is_fp_char(char ch) {
     return is_digit(ch) || ch == 'e' || ch == 'E' || ch == '-' || ch == '+' || ch == '.';
 }
 
-// pigo's read_fp on [p, e): returns the value and advances p (see the file comment)
-__device__ double parse_fp(const char*& p, const char* e, const double* __restrict__ pow10, int depth) {
+// pigo's read_fp on [p, e): returns the value and advances p (see the file comment).  pigo
+// raises the value to 10^exponent with std::pow for any exponent it reads, itself parsed by
+// read_fp (so "2e0.5" and "3e1e1" are numbers to it).  The table covers every integral exponent;
+// a line whose exponent is not an integer, or holds an exponent of its own, gets `host` set and
+// its value is computed again on the host with std::pow, as pigo does.
+__device__ double parse_fp(const char*& p, const char* e, const double* __restrict__ pow10, int depth,
+                           uint32_t& host) {
     double res = 0.0;
     while (p < e && !is_fp_char(*p)) ++p;
     bool positive = true;
@@ -104,12 +109,20 @@ __device__ double parse_fp(const char*& p, const char* e, const double* __restri
         const double scale = count <= kPow10Max ? pow10[count - kPow10Min] : INFINITY;
         res = __dadd_rn(res, __ddiv_rn(fraction, scale));
     }
-    if (p < e && (*p == 'e' || *p == 'E') && depth == 0) {
+    if (p < e && (*p == 'e' || *p == 'E')) {
+        if (depth > 0) {  // an exponent with an exponent of its own: pigo recurses; the host does it
+            host = 1;
+            return positive ? res : -res;
+        }
         ++p;
-        const double ex = parse_fp(p, e, pow10, 1);
-        const double k = fmin(fmax(ex, (double)kPow10Min), (double)kPow10Max);
-        if (k == ex && k == floor(k)) res = __dmul_rn(res, pow10[(int)k - kPow10Min]);
-        else res = __dmul_rn(res, ex > 0 ? INFINITY : 0.0);  // beyond double's range (or non-integral: unsupported)
+        const double ex = parse_fp(p, e, pow10, 1, host);
+        if (ex != floor(ex)) {
+            host = 1;  // non-integral (or NaN) exponent: std::pow on the host
+        } else {
+            const double k = fmin(fmax(ex, (double)kPow10Min), (double)kPow10Max);
+            // beyond the table, 10^ex is inf or 0 in double, as std::pow gives
+            res = __dmul_rn(res, k == ex ? pow10[(int)k - kPow10Min] : (ex > 0 ? INFINITY : 0.0));
+        }
     }
     return positive ? res : -res;
 }
@@ -118,7 +131,7 @@ __device__ double parse_fp(const char*& p, const char* e, const double* __restri
 __global__ void parse_lines_kernel(const char* __restrict__ buf, uint64_t n, const uint64_t* __restrict__ start,
                                    uint64_t nlines, uint32_t d, const double* __restrict__ pow10,
                                    uint32_t* __restrict__ idx, double* __restrict__ val, uint32_t* __restrict__ keep,
-                                   uint32_t* __restrict__ err) {
+                                   uint32_t* __restrict__ host_line, uint32_t* __restrict__ err) {
     const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= nlines) return;
     const char* p = buf + start[r];
@@ -157,7 +170,62 @@ __global__ void parse_lines_kernel(const char* __restrict__ buf, uint64_t n, con
         if (v == 0 || v > 0xffffffffull) atomicOr(err, 2u);  // labels are 1-based and fit 32 bits
         idx[r * d + m] = (uint32_t)(v - 1);
     }
-    val[r] = parse_fp(q, e, pow10, 0);
+    uint32_t host = 0;
+    val[r] = parse_fp(q, e, pow10, 0, host);
+    if (host) host_line[r] = 1;
+}
+
+// val[line[i]] = v[i]
+__global__ void patch_values_kernel(const uint64_t* __restrict__ line, const double* __restrict__ v, uint32_t n,
+                                    double* __restrict__ val) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) val[line[i]] = v[i];
+}
+
+bool host_fp_char(char ch) {
+    return (ch >= '0' && ch <= '9') || ch == 'e' || ch == 'E' || ch == '-' || ch == '+' || ch == '.';
+}
+
+// pigo's read_fp on the host (extern/pigo/pigo.hpp:2587-2627): integer and fraction parts
+// accumulated in double, res += fraction / std::pow(10, digits), then res *= std::pow(10, exp)
+// with the exponent read by the same routine.
+double host_read_fp(const char*& p, const char* e) {
+    double res = 0.0;
+    while (p < e && !host_fp_char(*p)) ++p;
+    bool positive = true;
+    if (p < e && *p == '-') {
+        positive = false;
+        ++p;
+    } else if (p < e && *p == '+') {
+        ++p;
+    }
+    while (p < e && *p >= '0' && *p <= '9') res = res * 10. + (double)(*p++ - '0');
+    if (p < e && *p == '.') {
+        ++p;
+        double fraction = 0.;
+        size_t count = 0;
+        while (p < e && *p >= '0' && *p <= '9') {
+            fraction = fraction * 10. + (double)(*p++ - '0');
+            ++count;
+        }
+        res += fraction / std::pow(10., (double)count);
+    }
+    if (p < e && (*p == 'e' || *p == 'E')) {
+        ++p;
+        const double ex = host_read_fp(p, e);
+        res *= std::pow(10., ex);
+    }
+    if (!positive) res *= -1;
+    return res;
+}
+
+// The value of data line [p, e) with d labels, by host_read_fp.
+double host_line_value(const char* p, const char* e, uint32_t d) {
+    for (uint32_t m = 0; m < d; ++m) {
+        while (p < e && !(*p >= '0' && *p <= '9')) ++p;
+        while (p < e && *p >= '0' && *p <= '9') ++p;
+    }
+    return host_read_fp(p, e);
 }
 
 __global__ void compact_lines_kernel(const uint32_t* __restrict__ idx, const double* __restrict__ val,
@@ -267,11 +335,41 @@ extern "C" ptc_status ptc_read_tns(const char* path, const ptc_options* opt_in, 
         uint32_t* keep = ar.alloc<uint32_t>(nlines + 1);
         uint32_t* err = ar.alloc<uint32_t>(1);
         PTC_CUDA(cudaMemsetAsync(err, 0, sizeof(uint32_t), st));
+        uint32_t* host_line = ar.alloc<uint32_t>(nlines);
+        PTC_CUDA(cudaMemsetAsync(host_line, 0, nlines * sizeof(uint32_t), st));
         const unsigned grid = (unsigned)((nlines + 255) / 256);
-        parse_lines_kernel<<<grid, 256, 0, st>>>(dbuf, n, start, nlines, d, pow10, tidx, tval, keep, err);
+        parse_lines_kernel<<<grid, 256, 0, st>>>(dbuf, n, start, nlines, d, pow10, tidx, tval, keep, host_line, err);
         PTC_CUDA(cudaGetLastError());
         uint32_t herr = 0;
         PTC_CUDA(cudaMemcpyAsync(&herr, err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        // lines whose exponent needs std::pow (non-integral or nested exponents; normally none)
+        uint64_t* nhost_d = ar.alloc<uint64_t>(1);
+        launch_sum_u32(host_line, nlines, nhost_d, st);
+        uint64_t nhost = 0;
+        PTC_CUDA(cudaMemcpyAsync(&nhost, nhost_d, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+        PTC_CUDA(cudaStreamSynchronize(st));
+        if (nhost > 0) {
+            std::vector<uint32_t> hl(nlines);
+            std::vector<uint64_t> hs(nlines + 1);
+            PTC_CUDA(cudaMemcpyAsync(hl.data(), host_line, nlines * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+            PTC_CUDA(cudaMemcpyAsync(hs.data(), start, nlines * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+            PTC_CUDA(cudaStreamSynchronize(st));
+            std::vector<uint64_t> lines;
+            std::vector<double> vals;
+            for (uint64_t r = 0; r < nlines; ++r) {
+                if (!hl[r]) continue;
+                const uint64_t e = r + 1 < nlines ? hs[r + 1] : n;
+                lines.push_back(r);
+                vals.push_back(host_line_value(host.data() + hs[r], host.data() + e, d));
+            }
+            uint64_t* dl = ar.alloc<uint64_t>(lines.size());
+            double* dvv = ar.alloc<double>(vals.size());
+            PTC_CUDA(cudaMemcpyAsync(dl, lines.data(), lines.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+            PTC_CUDA(cudaMemcpyAsync(dvv, vals.data(), vals.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+            patch_values_kernel<<<ceil_div_u32(lines.size(), 256), 256, 0, st>>>(dl, dvv, (uint32_t)lines.size(), tval);
+            PTC_CUDA(cudaGetLastError());
+            PTC_CUDA(cudaStreamSynchronize(st));  // the host vectors stay alive until the copies are done
+        }
 
         // 3. compact and mode sizes
         uint32_t* pos = ar.alloc<uint32_t>(nlines + 1);

@@ -36,13 +36,31 @@ CASES = [
 ]
 
 
-@pytest.mark.parametrize("case", CASES, ids=[f"c{i}" for i in range(len(CASES))])
-@pytest.mark.parametrize("panel", [0, 64, 4096])
-def test_against_oracle(engine, oracle_mod, case, panel):
-    dims, nnz, alphas, seed, values, c, modes = case
-    t = gen.random_coo(dims, nnz, alphas, seed, values)
-    o = oracle_mod.contract(t, None, c, modes)
-    idx, vals, st = engine.contract(t, None, c, modes, panel_width=panel)
+_ORACLE = {}
+
+
+def _case_and_oracle(oracle_mod, i):
+    """Case i's tensor and the restatement's output (computed once per test session)."""
+    if i not in _ORACLE:
+        dims, nnz, alphas, seed, values, c, modes = CASES[i]
+        t = gen.random_coo(dims, nnz, alphas, seed, values)
+        _ORACLE[i] = (t, oracle_mod.contract(t, None, c, modes))
+    return _ORACLE[i]
+
+
+# large-row accumulators: the row bitmap kernel, and the panel kernels (warp tasks and block
+# parts) at the automatic, narrowest and widest panel widths
+KERNELS = [("bitmap", 0), ("panels", 0), ("panels", 64), ("panels", 4096)]
+
+
+@pytest.mark.parametrize("case", range(len(CASES)), ids=[f"c{i}" for i in range(len(CASES))])
+@pytest.mark.parametrize("kernel", KERNELS, ids=[f"{k}{p}" for k, p in KERNELS])
+@pytest.mark.parametrize("path", ["two_phase", "learned"])
+def test_against_oracle(engine, oracle_mod, case, kernel, path):
+    t, o = _case_and_oracle(oracle_mod, case)
+    _, _, _, _, _, c, modes = CASES[case]
+    large_rows, panel = kernel
+    idx, vals, st = engine.contract(t, None, c, modes, panel_width=panel, large_rows=large_rows, path=path)
     assert st["mult_adds"] == o["flops"]
     assert st["nrows"] == o["nrows"] and st["nfibers"] == o["nfibers"]
     assert_same_output(idx, vals, o["idx"], o["vals"], bit_exact=True)

@@ -12,7 +12,10 @@ from partc_b200 import _lib, gen
 
 VALUE_TEXTS = ["0.5", "1", "-2.25", "3.14159265358979323846", "1e-3", "2.5E+2", "-7.0e1", "0.1", "123456789.987654321",
                "1.0000000000000002", "4.9e-300", "6.02214076e23", "+0.75", "0.000012345", "9.999999999999999e-1",
-               ".5", "42.", "0.30000000000000004"]
+               ".5", "42.", "0.30000000000000004",
+               # exponents pigo raises 10 to with std::pow although they are not integers, or that
+               # carry an exponent of their own (its read_fp reads the exponent recursively)
+               "2e0.5", "-3.5e-1.25", "1e1e1", "7E+0.125", "1.5e2.5e-1"]
 
 
 def _write_tricky(path, rng, n=4000):
