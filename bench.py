@@ -108,6 +108,16 @@ def host_info():
     return info
 
 
+def numeric_kernels(st):
+    """The kernels of the numeric pass a call ran (large rows on the row bitmap kernel report
+    panel width 0 and no parts)."""
+    if st["rows_hash"] > 0 and st["panel_width"] == 0 and st["hash_parts"] == 0:
+        large = "rowmap_kernel (one block per large row, column bitmap in shared memory)"
+    else:
+        large = "warp_task_kernel + hash_part_kernel (panel parts)"
+    return f"numeric pass: {large} + small_rows_kernel + copy_rows_kernel + esc_fold_kernel"
+
+
 def measured_hbm_peak():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -680,7 +690,7 @@ def main():
     traffic = traffic_from_profile()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": peak_kind,
-                "kernel": "numeric pass (warp_task_kernel + hash_part_kernel + small_rows_kernel<numeric>)",
+                "kernel": numeric_kernels(stats[0]),
                 "algorithmic_bytes": alg_bytes, "numeric_ms": t_num * 1e3,
                 "traffic": traffic.get("bytes_per_launch") if traffic else None}
 

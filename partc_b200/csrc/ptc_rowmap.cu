@@ -1,5 +1,6 @@
-// Large rows, one block per row over a bitmap of the row's columns in shared memory (the reference's numeric pass for rows with a hash SPA, fksCuckooTC.hpp:257-355,
-// and its per-row accumulator fksCuckooSPA.hpp, without a hash table).
+// Large rows, one block per row over a bitmap of the row's columns in shared memory (the
+// reference's numeric pass for rows with a hash SPA, fksCuckooTC.hpp:257-355, and its per-row
+// accumulator fksCuckooSPA.hpp, without a hash table).
 //
 // For one row the block
 //   A. sets a bit for the column of every product (any order): the distinct columns are the
@@ -85,6 +86,26 @@ __device__ __forceinline__ void apply_products(const Operands& op, uint32_t* wro
         if (dst[i]) __stcg(dst[i], add[i] ? __dadd_rn(old[i], p[i]) : p[i]);
 }
 
+constexpr uint32_t kRmUnit = 1024;  // fiber entries per unit of phase A
+
+// Fibers of A nonzeros kw .. kw + nk of a row into shared memory (thread t: nonzero kw + t):
+// start and length of the matching fiber (length 0 without one) and the A value.
+__device__ __forceinline__ void load_window(const Operands& op, uint32_t kw, uint32_t nk, uint32_t* ws, uint32_t* wl,
+                                            double* wa) {
+    const uint32_t t = threadIdx.x;
+    if (t < nk) {
+        const int32_t f = op.a_fib[kw + t];
+        uint32_t s = 0, L = 0;
+        if (f >= 0) {
+            s = op.fib_start[f];
+            L = op.fib_start[f + 1] - s;
+        }
+        ws[t] = s;
+        wl[t] = L;
+        wa[t] = op.a_val[kw + t];
+    }
+}
+
 template <int MODE, int FA, int FB>
 __global__ void __launch_bounds__(kRmThreads, 3)
     rowmap_kernel(Operands op, const uint32_t* __restrict__ rows, uint32_t nrows, uint64_t* __restrict__ row_d,
@@ -117,21 +138,34 @@ __global__ void __launch_bounds__(kRmThreads, 3)
         const uint32_t bitem = op.row_item ? op.row_item[row] : 0u;
         const uint32_t nw = (uint32_t)(((op.row_item ? (uint64_t)op.item_cols[bitem] : op.ncols) + 31) / 32);
 
-        // A. bitmap of the row's columns: warps over A nonzeros, lanes over fiber entries
-        for (uint32_t k = ka + warp; k < kb; k += kRmWarps) {
-            const int32_t f = op.a_fib[k];
-            if (f < 0) continue;
-            const uint32_t s = op.fib_start[f], e = op.fib_start[f + 1];
-            for (uint32_t j = s + lane; j < e; j += 32 * kRmUnroll) {
-                uint32_t c[kRmUnroll];
+        // A. bitmap of the row's columns.  A window of up to kRmThreads A nonzeros at a time: their
+        // fibers (start, length, A value) are read in parallel into shared memory, then every
+        // fiber is cut into units of kRmUnit entries that the warps take in turn (lanes over
+        // entries), so one long fiber does not hold the block up.
+        for (uint32_t kw = ka; kw < kb; kw += kRmThreads) {
+            const uint32_t nk = min((uint32_t)kRmThreads, kb - kw);
+            load_window(op, kw, nk, ws, wl, wa);
+            __syncthreads();
+            uint32_t unit = 0;
+            for (uint32_t i = 0; i < nk; ++i) {
+                const uint32_t L = wl[i], s = ws[i];
+                const uint32_t nu = (L + kRmUnit - 1) / kRmUnit;
+                for (uint32_t u = (warp + kRmWarps - unit % kRmWarps) % kRmWarps; u < nu; u += kRmWarps) {
+                    const uint32_t e = min(L, (u + 1) * kRmUnit);
+                    for (uint32_t j = u * kRmUnit + lane; j < e; j += 32 * kRmUnroll) {
+                        uint32_t c[kRmUnroll];
 #pragma unroll
-                for (int i = 0; i < kRmUnroll; ++i) c[i] = j + i * 32 < e ? __ldg(op.b_col + j + i * 32) : 0xffffffffu;
+                        for (int q = 0; q < kRmUnroll; ++q)
+                            c[q] = j + q * 32 < e ? __ldg(op.b_col + s + j + q * 32) : 0xffffffffu;
 #pragma unroll
-                for (int i = 0; i < kRmUnroll; ++i)
-                    if (c[i] != 0xffffffffu) atomicOr(&bits[c[i] >> 5], 1u << (c[i] & 31));
+                        for (int q = 0; q < kRmUnroll; ++q)
+                            if (c[q] != 0xffffffffu) atomicOr(&bits[c[q] >> 5], 1u << (c[q] & 31));
+                    }
+                }
+                unit += nu;
             }
+            __syncthreads();
         }
-        __syncthreads();
 
         // B. word prefixes: thread t takes words [t * per, (t + 1) * per)
         const uint32_t per = (nw + kRmThreads - 1) / kRmThreads;
@@ -181,18 +215,10 @@ __global__ void __launch_bounds__(kRmThreads, 3)
                 // C. products, one A nonzero after the other
                 for (uint32_t kw = ka; kw < kb; kw += kRmThreads) {
                     const uint32_t nk = min((uint32_t)kRmThreads, kb - kw);
-                    if (t < nk) {
-                        const int32_t f = op.a_fib[kw + t];
-                        uint32_t s = 0, L = 0;
-                        if (f >= 0) {
-                            s = op.fib_start[f];
-                            L = op.fib_start[f + 1] - s;
-                        }
-                        ws[t] = s;
-                        wl[t] = L;
-                        wa[t] = op.a_val[kw + t];
+                    if (kb - ka > kRmThreads) {  // (a row of one window still has it from phase A)
+                        load_window(op, kw, nk, ws, wl, wa);
+                        __syncthreads();
                     }
-                    __syncthreads();
                     for (uint32_t i = 0; i < nk;) {
                         const uint32_t L = wl[i];
                         if (L >= kShortFiber) {
