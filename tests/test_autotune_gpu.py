@@ -22,8 +22,9 @@ def test_autotune_picks_knobs_and_results_stay_exact(engine, oracle_mod):
         assert_same_output(idx, vals, o["idx"], o["vals"], bit_exact=True)
 
 
-@pytest.mark.parametrize("knobs", [dict(panel_width=64, warp_task_max_len=1), dict(small_max_products=128,
-                                   sort_max_avg_products=64, hash_load_pct=50), dict(panel_width=1024)])
+@pytest.mark.parametrize("knobs", [dict(large_rows="panels", panel_width=64, warp_task_max_len=1),
+                                   dict(small_max_products=128, sort_max_avg_products=64, hash_load_pct=50),
+                                   dict(large_rows="panels", panel_width=1024), dict(large_rows="bitmap")])
 def test_every_knob_setting_gives_the_same_result(engine, oracle_mod, knobs):
     t = gen.random_coo([300, 200, 40], 60000, [1.3, 1.0, 1.1], 13, "uniform11")
     o = oracle_mod.contract(t, None, 1, [2, 0, 1])
