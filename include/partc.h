@@ -318,12 +318,12 @@ ptc_status ptc_sizer_predict(const ptc_sizer* s, const float* features, uint64_t
  * owns the device, or an allocation would synchronize the device or is not allowed there).  Its
  * device scratch -- the BF16 weights, up to 65536 staged feature rows and their predictions -- is
  * one static device array of about 4.3 MiB that every device loading the library keeps until the
- * process exits.  n > 65536 is rejected with PTC_ERR_INVALID_ARGUMENT.  Every call looks up that
- * array's address on the device (an allocation-free lookup); the first call on a device also loads
- * the library's device code there, so make it before capturing any stream.  All calls share the
- * array: calls whose GPU work overlaps race on it.  Runs on the calling thread's per-thread
- * default stream, restores the caller's current device and returns when out holds the
- * predictions (host arrays in and out). */
+ * process exits.  n > 65536 is rejected with PTC_ERR_INVALID_ARGUMENT.  The first call on a device
+ * looks up that array's address there and keeps it; make that call before capturing any stream
+ * (the kept address does not survive a cudaDeviceReset of the device).  All calls share the array:
+ * calls whose GPU work overlaps race on it.  Runs on the calling thread's per-thread default
+ * stream, restores the caller's current device and returns when out holds the predictions (host
+ * arrays in and out). */
 ptc_status ptc_sizer_predict_noalloc(const ptc_sizer* s, const float* features, uint64_t n,
                                      int32_t device, float* out);
 /* Gradient of the mean squared error over n samples (host arrays; grads has PTC_SIZER_PARAMS). */

@@ -12,10 +12,11 @@
 // Rules for callers:
 //   * at most kNoAllocMaxRows feature rows per call; a larger call is rejected with
 //     PTC_ERR_INVALID_ARGUMENT and does nothing;
-//   * every call looks up the array's device address (cudaGetSymbolAddress, which allocates
-//     nothing) with the device current, so the address stays right after a cudaDeviceReset; the
-//     first call on a device also loads the library's device code there, so make that first call
-//     before capturing any stream;
+//   * the first call on a device looks up the array's device address there (cudaGetSymbolAddress,
+//     once per device, with that device current) and keeps it for the life of the process; make
+//     that first call before capturing any stream.  The kept address does not survive a
+//     cudaDeviceReset of that device: after a reset this entry point must not be called again in
+//     the same process;
 //   * the caller's current device is restored before the call returns;
 //   * every call uses the same array and overwrites it; nothing in it needs to start at zero, since
 //     each call writes every byte it later reads.  Calls whose GPU work overlaps (two host threads,
@@ -24,6 +25,7 @@
 #include <cuda_bf16.h>
 
 #include <cstring>
+#include <mutex>
 
 #include "partc.h"
 #include "ptc_sizer.cuh"
@@ -47,13 +49,23 @@ constexpr size_t kNoAllocScratchBytes = align256(kOffY + kNoAllocMaxRows * sizeo
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-// Device address of the scratch array on the current device.  Looked up on every call: the
-// lookup allocates nothing, and an address kept from before a cudaDeviceReset would be stale.
-unsigned char* scratch_on_current_device() {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) throw Error{PTC_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e)};
-    return static_cast<unsigned char*>(p);
+constexpr int kMaxDevices = 64;
+std::mutex g_mu;
+unsigned char* g_scratch_ptr[kMaxDevices] = {};
+
+// Device address of the scratch array on `device` (which must be current), looked up on the
+// first call there.  In host code the array's name only stands for it; the kernel needs this.
+unsigned char* scratch_on(int device) {
+    PTC_REQUIRE(device >= 0 && device < kMaxDevices, PTC_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (!g_scratch_ptr[device]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess)
+            throw Error{PTC_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e)};
+        g_scratch_ptr[device] = static_cast<unsigned char*>(p);
+    }
+    return g_scratch_ptr[device];
 }
 
 // The network's forward pass (the same arithmetic as the sizer's inference kernel), reading the
@@ -120,7 +132,8 @@ extern "C" ptc_status ptc_sizer_predict_noalloc(const ptc_sizer* s, const float*
             throw Error{PTC_ERR_NO_DEVICE, "no usable CUDA device"};
         }
         if (device >= 0) PTC_CUDA(cudaSetDevice(device));
-        unsigned char* base = scratch_on_current_device();
+        else PTC_CUDA(cudaGetDevice(&device));
+        unsigned char* base = scratch_on(device);
         if (n == 0) return PTC_OK;
         // the weights as the device uses them: W1, W2, w3 in BF16, biases in FP32 (host staging
         // on the stack; no allocation)
