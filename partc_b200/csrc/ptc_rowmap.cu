@@ -245,40 +245,51 @@ __global__ void __launch_bounds__(kRmThreads, 3)
                     }
                 }
 
-                // D. index tuples in column order: thread per word, consecutive words per warp
+                // D. index tuples in column order.  Entry o of the row holds column c.
                 uint32_t rt[FA > 0 ? FA : 1];
                 if (FA > 0)
                     for (int m = 0; m < FA; ++m) rt[m] = op.row_tuple[(uint64_t)row * FA + m];
-                for (uint32_t w = t; w < nw; w += kRmThreads) {
-                    uint32_t m = bits[w];
-                    uint64_t o = pref[w];  // entry of the row
-                    while (m) {
-                        const uint32_t c = (w << 5) | (uint32_t)(__ffs(m) - 1);
-                        m &= m - 1;
-                        if (FA > 0) {
-                            uint32_t* dst = out.idx + ibase + o * (FA + FB);
-                            if (FA == 2 && FB == 2) {
-                                const uint2 ct = *reinterpret_cast<const uint2*>(op.col_tuple + (uint64_t)c * 2);
-                                __stcs(reinterpret_cast<uint4*>(dst), make_uint4(rt[0], rt[1], ct.x, ct.y));
-                            } else if (FA == 1 && FB == 1) {
-                                __stcs(reinterpret_cast<uint2*>(dst), make_uint2(rt[0], op.col_tuple[c]));
-                            } else {
-                                for (int q = 0; q < FA; ++q) dst[q] = rt[q];
-                                for (int q = 0; q < FB; ++q) dst[FA + q] = op.col_tuple[(uint64_t)c * FB + q];
-                            }
+                auto write_tuple = [&](uint64_t o, uint32_t c) {
+                    if (FA > 0) {
+                        uint32_t* dst = out.idx + ibase + o * (FA + FB);
+                        if (FA == 2 && FB == 2) {
+                            const uint2 ct = *reinterpret_cast<const uint2*>(op.col_tuple + (uint64_t)c * 2);
+                            __stcs(reinterpret_cast<uint4*>(dst), make_uint4(rt[0], rt[1], ct.x, ct.y));
+                        } else if (FA == 1 && FB == 1) {
+                            __stcs(reinterpret_cast<uint2*>(dst), make_uint2(rt[0], op.col_tuple[c]));
                         } else {
-                            // any order; in a batch the row and column tuples are stored with
-                            // the batch's widest strides (op.fa, op.fb), the entry with the item's
-                            uint32_t* dst = out.idx + ibase + o * (ifa + ifb);
-                            const uint32_t cg = c + colbase;
-                            for (uint32_t q = 0; q < ifa; ++q) dst[q] = op.row_tuple[(uint64_t)row * op.fa + q];
-                            for (uint32_t q = 0; q < ifb; ++q) dst[ifa + q] = op.col_tuple[(uint64_t)cg * op.fb + q];
+                            for (int q = 0; q < FA; ++q) dst[q] = rt[q];
+                            for (int q = 0; q < FB; ++q) dst[FA + q] = op.col_tuple[(uint64_t)c * FB + q];
                         }
-                        if (out.row_of) {
-                            out.row_of[base + o] = row;
-                            out.col_of[base + o] = c;
+                    } else {
+                        // any order; in a batch the row and column tuples are stored with the
+                        // batch's widest strides (op.fa, op.fb), the entry with the item's
+                        uint32_t* dst = out.idx + ibase + o * (ifa + ifb);
+                        const uint32_t cg = c + colbase;
+                        for (uint32_t q = 0; q < ifa; ++q) dst[q] = op.row_tuple[(uint64_t)row * op.fa + q];
+                        for (uint32_t q = 0; q < ifb; ++q) dst[ifa + q] = op.col_tuple[(uint64_t)cg * op.fb + q];
+                    }
+                    if (out.row_of) {
+                        out.row_of[base + o] = row;
+                        out.col_of[base + o] = c;
+                    }
+                };
+                if ((uint64_t)count * 2 > (uint64_t)nw * 32) {
+                    // a dense row: a warp per bitmap word, lanes over its bits, so the set lanes
+                    // write consecutive entries
+                    for (uint32_t w = warp; w < nw; w += kRmWarps) {
+                        const uint32_t m = bits[w];
+                        if ((m >> lane) & 1u) write_tuple(pref[w] + __popc(m & lanemask_lt()), (w << 5) | lane);
+                    }
+                } else {
+                    // a sparse row: a thread per word (consecutive words per warp), its set bits in turn
+                    for (uint32_t w = t; w < nw; w += kRmThreads) {
+                        uint32_t m = bits[w];
+                        uint64_t o = pref[w];
+                        while (m) {
+                            write_tuple(o++, (w << 5) | (uint32_t)(__ffs(m) - 1));
+                            m &= m - 1;
                         }
-                        ++o;
                     }
                 }
             }
