@@ -113,13 +113,17 @@ typedef struct ptc_options {
                                        failures, twice the buckets (the reference's rehash with new
                                        kDict pairs and a larger table, fksCuckoo.hpp:297-442), before
                                        the call returns PTC_ERR_HASH_BUILD (default 8) */
-    uint32_t large_rows;            /* accumulator of the large rows of a single contraction:
-                                       PTC_LARGE_ROWS_AUTO (0, default: the row bitmap when the
-                                       columns fit it), PTC_LARGE_ROWS_BITMAP (one block per row,
-                                       a bitmap of its columns in shared memory, up to about 600k
-                                       distinct B free keys) or PTC_LARGE_ROWS_PANELS (warp tasks
-                                       and block parts over column panels, any size) */
-    uint32_t reserved[1];
+    uint32_t large_rows;            /* accumulator of the large rows: PTC_LARGE_ROWS_AUTO (0,
+                                       default: rows of at most bitmap_max_len A nonzeros on the
+                                       row bitmap kernel when the columns fit it, the others on the
+                                       panel kernels), PTC_LARGE_ROWS_BITMAP (every large row on the
+                                       row bitmap kernel -- one block per row, a bitmap of its
+                                       columns in shared memory, up to about 600k distinct B free
+                                       keys) or PTC_LARGE_ROWS_PANELS (warp tasks and block parts
+                                       over column panels, any size) */
+    uint32_t bitmap_max_len;        /* PTC_LARGE_ROWS_AUTO: A nonzeros of the longest row on the
+                                       row bitmap kernel (default 64) */
+    uint32_t reserved[2];
 } ptc_options;
 
 enum { PTC_LARGE_ROWS_AUTO = 0, PTC_LARGE_ROWS_BITMAP = 1, PTC_LARGE_ROWS_PANELS = 2 };

@@ -62,7 +62,8 @@ class Options(C.Structure):
                 ("sort_rows", C.c_uint32), ("small_max_products", C.c_uint32),
                 ("sort_max_avg_products", C.c_uint32), ("hash_load_pct", C.c_uint32),
                 ("batch_wave_mib", C.c_uint32), ("warp_task_max_len", C.c_uint32), ("cuckoo_max_chain", C.c_uint32),
-                ("cuckoo_max_attempts", C.c_uint32), ("large_rows", C.c_uint32), ("reserved", C.c_uint32 * 1)]
+                ("cuckoo_max_attempts", C.c_uint32), ("large_rows", C.c_uint32), ("bitmap_max_len", C.c_uint32),
+                ("reserved", C.c_uint32 * 2)]
 
 
 class Stats(C.Structure):
@@ -93,7 +94,7 @@ class TuneReport(C.Structure):
     _fields_ = [("trials", C.c_uint32), ("repeats", C.c_uint32), ("default_ms", C.c_double),
                 ("best_ms", C.c_double), ("reserved", C.c_double * 4)]
 
-TUNE_KNOBS = ("large_rows", "panel_width", "warp_task_max_len", "small_max_products", "sort_max_avg_products",
+TUNE_KNOBS = ("large_rows", "bitmap_max_len", "panel_width", "warp_task_max_len", "small_max_products", "sort_max_avg_products",
               "hash_load_pct")
 
 

@@ -586,14 +586,12 @@ struct Launched {
 // accumulator overflowed or whose claim did not fit wrote nothing and are listed in their launch's
 // fail list.  Their rows get the exact symbolic pass, each failed item is re-split exactly into
 // block parts, and those claim after the entries already written (their sizes are exact, so they
-// cannot fail again).  Returns the output nnz.
-uint64_t learned_reruns(const Operands& op, std::vector<Launched> groups, const uint32_t* big_rows, uint32_t n_big,
-                        const float* pred, const SplitRule& rule, OutputView& ov, uint32_t* work_counter,
-                        uint32_t* err, int num_sms, uint64_t nrows, Arena& ar, ptc_stats& stats) {
+// cannot fail again).  Adds every row's entries to row_actual; returns the rows rerun.
+uint64_t learned_reruns(const Operands& op, std::vector<Launched> groups, const SplitRule& rule, OutputView& ov,
+                        uint32_t* work_counter, uint32_t* err, int num_sms, uint64_t nrows, uint64_t* row_actual,
+                        Arena& ar) {
     cudaStream_t st = ar.stream();
     const uint32_t P = op.npanels;
-    uint64_t* row_actual = ar.alloc<uint64_t>(nrows);
-    PTC_CUDA(cudaMemsetAsync(row_actual, 0, nrows * sizeof(uint64_t), st));
     for (const Launched& g : groups) launch_row_actual(g.parts, g.item_count, g.n, row_actual, st);
     uint64_t rerun_rows = 0;
     for (int round = 0;; ++round) {
@@ -651,30 +649,18 @@ uint64_t learned_reruns(const Operands& op, std::vector<Launched> groups, const 
         launch_row_actual(fresh, g.item_count, nnew, row_actual, st);
         groups.assign(1, g);
     }
-    stats.rerun_rows = rerun_rows;
-    double* esum = ar.alloc<double>(1);
-    launch_log2_error(big_rows, n_big, pred, row_actual, esum, st);
-    stats.sizer_mean_abs_log2_err = n_big ? read_scalar(esum, st) / n_big : 0.0;
-    return read_scalar(ov.cursor, st) - read_scalar(ov.overshoot, st);
+    return rerun_rows;
 }
 
 // Learned path on the row bitmap kernel: rows whose claim did not fit the predicted output are
 // listed in mo.fail_list (their exact counts in mo.item_count); the output grows to hold them
 // and they run again, claiming after the entries already written (their sizes are now known, so
-// they cannot fail again).  Returns the output nnz.
-uint64_t rowmap_reruns(const Operands& op, const uint32_t* rows, uint32_t nrows, const float* pred,
-                       const OutputView& mo, OutputView& ov, uint32_t* work_counter, int num_sms, Arena& ar,
-                       ptc_stats& stats) {
+// they cannot fail again).  Writes every row's entries to row_actual; returns the rows rerun.
+uint64_t rowmap_reruns(const Operands& op, const uint32_t* rows, uint32_t nrows, const OutputView& mo,
+                       OutputView& ov, uint32_t* work_counter, int num_sms, uint64_t* row_actual, Arena& ar) {
     cudaStream_t st = ar.stream();
     const uint32_t nfail = read_scalar(mo.fail_count, st);
-    if (nrows > 0) {  // the sizer's error over the rows it sized (every row's exact count is known)
-        uint64_t* row_actual = ar.alloc<uint64_t>(op.nrows);
-        launch_scatter_counts(rows, nrows, mo.item_count, row_actual, st);
-        double* esum = ar.alloc<double>(1);
-        launch_log2_error(rows, nrows, pred, row_actual, esum, st);
-        stats.sizer_mean_abs_log2_err = read_scalar(esum, st) / nrows;
-    }
-    stats.rerun_rows = nfail;
+    launch_scatter_counts(rows, nrows, mo.item_count, row_actual, st);
     if (nfail > 0) {
         uint32_t* again = ar.alloc<uint32_t>(nfail);
         uint32_t* cnt = ar.alloc<uint32_t>(nfail);
@@ -695,7 +681,7 @@ uint64_t rowmap_reruns(const Operands& op, const uint32_t* rows, uint32_t nrows,
         launch_rowmap(kRowmapClaim, op, again, nfail, nullptr, nullptr, o2, work_counter, num_sms, st);
         PTC_REQUIRE(read_scalar(o2.fail_count, st) == 0, PTC_ERR_INTERNAL, "exactly sized rows failed again");
     }
-    return read_scalar(ov.cursor, st) - read_scalar(ov.overshoot, st);
+    return nfail;
 }
 
 // Training samples of the learned sizer, gathered instead of running the numeric pass.
@@ -760,6 +746,8 @@ struct Plan {
     uint64_t* esc_run_key = nullptr;
     uint32_t* esc_run_start = nullptr;
     uint32_t* esc_first = nullptr;  // [n_esc + 1] first run of each sort-based row
+    uint32_t* esc_long = nullptr;   // the runs of at least kEscLongMin products, increasing
+    std::vector<uint32_t> h_esc_long;
     double* esc_sorted = nullptr;   // products in run order
     // sizes: exact offsets of the small and sort-based rows (and, on the two-phase path, of every
     // row); the learned path's large rows claim instead, within claim_off's budgets
@@ -782,7 +770,8 @@ struct Plan {
     bool collected = false;
     // large rows of a single contraction on the row bitmap kernel (instead of parts): the rows
     // it writes, heaviest first (the two-phase path leaves the collision-free rows to copy_rows)
-    bool rowmap = false;
+    bool rowmap = false;      // every large row is on the row bitmap kernel (no panels at all)
+    uint32_t n_mapped = 0;    // big_rows[0, n_mapped): the large rows on the row bitmap kernel
     uint32_t* map_rows = nullptr;
     uint32_t n_map = 0;
 };
@@ -853,27 +842,35 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
     launch_compact_indices(small_flag, pl.small_pos, nrows, pl.small_rows, st);
     launch_compact_indices(big_flag, big_pos, nrows, pl.big_rows, st);
     const uint32_t n_small = pl.n_small, n_big = pl.n_big, n_esc = pl.n_esc;
-    // large rows: warp tasks for rows of at most kWarpTaskMaxLen A nonzeros (panels of at most
-    // a dense warp task's width), block parts for the others; each group largest first
-    // the row bitmap kernel takes every large row of a single contraction whose columns fit it
-    // (a batch's columns are its items' own: the widest item decides)
-    pl.rowmap = opt.large_rows != PTC_LARGE_ROWS_PANELS && ncols <= rowmap_max_cols();
-    PTC_REQUIRE(!(opt.large_rows == PTC_LARGE_ROWS_BITMAP && !pl.rowmap), PTC_ERR_INVALID_ARGUMENT,
+    // large rows, three groups, each largest first: the row bitmap kernel takes rows of at most
+    // map_len A nonzeros (its barrier rounds, one per A nonzero, stay few), when the columns fit
+    // its bitmap (a batch's columns are its items' own: the widest item decides); warp tasks the
+    // next rows up to warp_len A nonzeros (panels of at most a dense warp task's width); block
+    // parts the others
+    const bool bitmap_ok = opt.large_rows != PTC_LARGE_ROWS_PANELS && ncols <= rowmap_max_cols();
+    PTC_REQUIRE(!(opt.large_rows == PTC_LARGE_ROWS_BITMAP && !bitmap_ok), PTC_ERR_INVALID_ARGUMENT,
                 "large_rows = PTC_LARGE_ROWS_BITMAP: at most about 600k distinct B free keys per contraction");
-    const uint32_t warp_len = pl.rowmap ? UINT32_MAX
-                              : (opt.panel_width == 0 || opt.panel_width <= warp_task_dense_columns())
+    const uint32_t map_len = !bitmap_ok ? 0u
+                             : opt.large_rows == PTC_LARGE_ROWS_BITMAP ? UINT32_MAX
+                             : (opt.bitmap_max_len ? opt.bitmap_max_len : kBitmapMaxLen);
+    const uint32_t warp_len = (opt.panel_width == 0 || opt.panel_width <= warp_task_dense_columns())
                                   ? (opt.warp_task_max_len ? opt.warp_task_max_len : kWarpTaskMaxLen) : 0u;
     if (n_big > 0) {
         uint64_t* wkey = ar.alloc<uint64_t>(n_big);
-        launch_work_keys(pl.big_rows, n_big, pl.row_flops, op.row_start, warp_len, wkey, st);
-        if (n_big > 1) radix_sort_pairs(wkey, pl.big_rows, n_big, 0, 41, ar);
-        const uint64_t split = 1ull << 40;
-        uint64_t* split_d = ar.alloc<uint64_t>(1);
-        uint32_t* first = ar.alloc<uint32_t>(2);
-        PTC_CUDA(cudaMemcpyAsync(split_d, &split, sizeof(uint64_t), cudaMemcpyHostToDevice, st));
-        launch_key_bounds(wkey, n_big, split_d, 1, first, st);
-        pl.n_warp_rows = read_scalar(first, st);
+        launch_work_keys(pl.big_rows, n_big, pl.row_flops, op.row_start, map_len, warp_len, wkey, st);
+        if (n_big > 1) radix_sort_pairs(wkey, pl.big_rows, n_big, 0, 42, ar);
+        const uint64_t split[2] = {1ull << 40, 2ull << 40};
+        uint64_t* split_d = ar.alloc<uint64_t>(2);
+        uint32_t* first = ar.alloc<uint32_t>(3);
+        PTC_CUDA(cudaMemcpyAsync(split_d, split, 2 * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+        launch_key_bounds(wkey, n_big, split_d, 2, first, st);
+        uint32_t hf[2];
+        PTC_CUDA(cudaMemcpyAsync(hf, first, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        PTC_CUDA(cudaStreamSynchronize(st));
+        pl.n_mapped = hf[0];
+        pl.n_warp_rows = hf[1] - hf[0];
     }
+    pl.rowmap = n_big > 0 && pl.n_mapped == n_big;
     stats.rows_small = n_small;
     stats.rows_hash = n_big;
     stats.rows_long = n_esc;
@@ -971,9 +968,10 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
     OutputView none;
     launch_small_rows(false, op, pl.small_rows, n_small, row_d, nullptr, none, st);
     if (!pl.learned) {
-        if (pl.rowmap) launch_rowmap(kRowmapCount, op, pl.big_rows, n_big, row_d, nullptr, none, pl.work_counter,
-                                     num_sms, st);
-        else launch_sym_bitmap(op, pl.big_rows, n_big, panel_cnt, pbase, row_d, pl.work_counter, num_sms, st);
+        const uint32_t nm = pl.n_mapped;
+        launch_rowmap(kRowmapCount, op, pl.big_rows, nm, row_d, nullptr, none, pl.work_counter, num_sms, st);
+        launch_sym_bitmap(op, pl.big_rows + nm, n_big - nm, pbase ? panel_cnt : panel_cnt + (uint64_t)nm * P,
+                          pbase ? pbase + nm : nullptr, row_d, pl.work_counter, num_sms, st);
     }
     // sort-based rows: expand their products in stream order, sort stably by (row, column)
     pl.esc_colbits = (uint32_t)colbits;
@@ -991,6 +989,21 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
         pl.esc_runs = runs_of_sorted(esc_key, f_esc, nullptr, pl.esc_run_start, pl.esc_run_key, ar);
         pl.esc_first = ar.alloc<uint32_t>((uint64_t)n_esc + 1);
         launch_esc_count(pl.esc_run_key, pl.esc_runs, pl.esc_colbits, pl.esc_rows, row_d, pl.esc_first, st);
+        {  // long runs: folded a block each
+            uint32_t* flag = ar.alloc<uint32_t>(pl.esc_runs + 1);
+            uint32_t* pos = ar.alloc<uint32_t>(pl.esc_runs + 1);
+            launch_esc_long_flags(pl.esc_run_start, pl.esc_runs, flag, st);
+            exclusive_scan<uint32_t>(flag, pos, pl.esc_runs, ar);
+            const uint32_t nl = read_scalar(pos + pl.esc_runs, st);
+            if (nl > 0) {
+                pl.esc_long = ar.alloc<uint32_t>(nl);
+                launch_compact_indices(flag, pos, pl.esc_runs, pl.esc_long, st);
+                pl.h_esc_long.resize(nl);
+                PTC_CUDA(cudaMemcpyAsync(pl.h_esc_long.data(), pl.esc_long, nl * sizeof(uint32_t),
+                                         cudaMemcpyDeviceToHost, st));
+                PTC_CUDA(cudaStreamSynchronize(st));
+            }
+        }
         const uint32_t total_runs = (uint32_t)pl.esc_runs;
         PTC_CUDA(cudaMemcpyAsync(pl.esc_first + n_esc, &total_runs, sizeof(uint32_t), cudaMemcpyHostToDevice, st));
         // the products in run order (the sort keys are no longer needed: their buffer takes them)
@@ -1084,29 +1097,33 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
         }
     }
 
-    if (pl.rowmap) {
-        // the rows the bitmap kernel writes: every large row but the collision-free ones, in
+    {
+        // the rows the bitmap kernel writes: its large rows but the collision-free ones, in
         // big_rows' heaviest-first order
+        const uint32_t nm = pl.n_mapped;
         pl.map_rows = pl.big_rows;
-        pl.n_map = n_big;
-        if (skip_off && n_big > 0 && pl.n_copy > 0) {
-            uint32_t* flag = ar.alloc<uint32_t>((uint64_t)n_big + 1);
-            uint32_t* pos = ar.alloc<uint32_t>((uint64_t)n_big + 1);
-            launch_table_row_flags(pl.big_rows, n_big, skip_off, skip_flops, flag, st);
-            exclusive_scan<uint32_t>(flag, pos, n_big, ar);
-            pl.n_map = read_scalar(pos + n_big, st);
+        pl.n_map = nm;
+        if (skip_off && nm > 0 && pl.n_copy > 0) {
+            uint32_t* flag = ar.alloc<uint32_t>((uint64_t)nm + 1);
+            uint32_t* pos = ar.alloc<uint32_t>((uint64_t)nm + 1);
+            launch_table_row_flags(pl.big_rows, nm, skip_off, skip_flops, flag, st);
+            exclusive_scan<uint32_t>(flag, pos, nm, ar);
+            pl.n_map = read_scalar(pos + nm, st);
             uint32_t* sel = ar.alloc<uint32_t>(std::max<uint32_t>(pl.n_map, 1));
-            launch_compact_indices(flag, pos, n_big, sel, st);
+            launch_compact_indices(flag, pos, nm, sel, st);
             pl.map_rows = ar.alloc<uint32_t>(std::max<uint32_t>(pl.n_map, 1));
             launch_gather<uint32_t>(pl.big_rows, sel, pl.n_map, pl.map_rows, st);
         }
+    }
+    if (pl.rowmap) {
         stats.hash_parts = 0;
         return pl;
     }
 
-    // split large rows into tasks / parts that fit a shared-memory table
+    // split the other large rows into tasks / parts that fit a shared-memory table
     for (int kind = 0; kind < 2; ++kind) {
-        const uint64_t r0 = kind == 0 ? 0 : pl.n_warp_rows, nr = kind == 0 ? pl.n_warp_rows : n_big - pl.n_warp_rows;
+        const uint64_t r0 = kind == 0 ? pl.n_mapped : pl.n_mapped + pl.n_warp_rows;
+        const uint64_t nr = kind == 0 ? pl.n_warp_rows : n_big - r0;
         uint32_t* nparts = ar.alloc<uint32_t>(nr + 1);
         const uint32_t* pc = pbase ? panel_cnt : panel_cnt + r0 * P;
         const uint64_t* pb = pbase ? pbase + r0 : nullptr;
@@ -1274,7 +1291,7 @@ void contract_impl(const ptc_coo* A, const ptc_coo* Bin, uint32_t c, const uint3
         launch_small_rows(true, op, pl.small_rows, pl.n_small, nullptr, pl.row_off, ov, st);
         launch_copy_rows(op, pl.copy_rows, pl.n_copy, pl.alen, pl.row_off, ov, dev.num_sms, st);
         OutputView mo = ov;  // the row bitmap kernel's view (claim bookkeeping on the learned path)
-        if (pl.rowmap) {
+        if (pl.n_map > 0) {
             if (learned) {
                 const uint32_t n = std::max<uint32_t>(pl.n_map, 1);
                 mo.fail_count = ar.alloc<uint32_t>(1);
@@ -1285,7 +1302,7 @@ void contract_impl(const ptc_coo* A, const ptc_coo* Bin, uint32_t c, const uint3
             launch_rowmap(learned ? kRowmapClaim : kRowmapExact, op, pl.map_rows, pl.n_map, nullptr, pl.row_off, mo,
                           pl.work_counter, dev.num_sms, st);
         }
-        for (int kind = 0; kind < 2 && !pl.rowmap; ++kind) {
+        for (int kind = 0; kind < 2; ++kind) {
             OutputView o = ov;
             if (learned) {
                 const uint32_t n = std::max<uint32_t>(pl.n_parts[kind], 1);
@@ -1298,13 +1315,23 @@ void contract_impl(const ptc_coo* A, const ptc_coo* Bin, uint32_t c, const uint3
             launch_parts(kind, op, pl.parts[kind], pl.n_parts[kind], o, pl.work_counter, op.err, dev.num_sms, st);
         }
         launch_esc_fold(op, ov, pl.esc_run_key, pl.esc_run_start, 0, pl.esc_runs, pl.esc_colbits, pl.esc_rows,
-                        pl.esc_first, pl.row_off, pl.esc_sorted, st);
-        if (learned && pl.rowmap) {
-            out_nnz = rowmap_reruns(op, pl.map_rows, pl.n_map, pl.pred, mo, ov, pl.work_counter, dev.num_sms, ar,
-                                    stats);
-        } else if (learned) {
-            out_nnz = learned_reruns(op, groups, pl.big_rows, pl.n_big, pl.pred, pl.rule[1], ov, pl.work_counter,
-                                     op.err, dev.num_sms, op.nrows, ar, stats);
+                        pl.esc_first, pl.row_off, pl.esc_sorted, pl.esc_long,
+                        (uint32_t)pl.h_esc_long.size(), st);
+        if (learned) {
+            // rows whose prediction fell short run again exactly (parts first, then the bitmap
+            // kernel's rows; each grows the output as needed), and the sizer's error over the large
+            // rows, every one of whose exact counts is known by now
+            uint64_t* row_actual = ar.alloc<uint64_t>(std::max<uint64_t>(op.nrows, 1));
+            PTC_CUDA(cudaMemsetAsync(row_actual, 0, std::max<uint64_t>(op.nrows, 1) * sizeof(uint64_t), st));
+            stats.rerun_rows = learned_reruns(op, groups, pl.rule[1], ov, pl.work_counter, op.err, dev.num_sms,
+                                              op.nrows, row_actual, ar);
+            if (pl.n_map > 0)
+                stats.rerun_rows += rowmap_reruns(op, pl.map_rows, pl.n_map, mo, ov, pl.work_counter, dev.num_sms,
+                                                  row_actual, ar);
+            double* esum = ar.alloc<double>(1);
+            launch_log2_error(pl.big_rows, pl.n_big, pl.pred, row_actual, esum, st);
+            stats.sizer_mean_abs_log2_err = pl.n_big ? read_scalar(esum, st) / pl.n_big : 0.0;
+            out_nnz = read_scalar(ov.cursor, st) - read_scalar(ov.overshoot, st);
         }
         if (opt.sort_rows && out_nnz > 1) {
             // rows in increasing free-key order, every row in increasing column order: one sort
@@ -1762,7 +1789,7 @@ void batch_impl(const std::vector<BatchItemHost>& items, uint32_t location, cons
     const uint32_t* map_rows = pl.map_rows;
     std::vector<uint32_t> mb(nw + 1, 0);
     mb[nw] = pl.n_map;
-    if (pl.rowmap && nw > 1 && pl.n_map > 0) {
+    if (nw > 1 && pl.n_map > 0) {
         uint64_t* key = ar.alloc<uint64_t>(pl.n_map);
         uint32_t* idx = ar.alloc<uint32_t>(pl.n_map);
         launch_row_wave(pl.map_rows, pl.n_map, wave_row_d, nw, key, idx, st);
@@ -1777,7 +1804,7 @@ void batch_impl(const std::vector<BatchItemHost>& items, uint32_t location, cons
     }
     uint32_t* map_fail_count = nullptr;
     uint32_t* map_fail_list = nullptr;
-    if (learned && pl.rowmap) {
+    if (learned && pl.n_map > 0) {
         map_fail_count = ar.alloc<uint32_t>(1);
         map_fail_list = ar.alloc<uint32_t>(std::max<uint32_t>(pl.n_map, 1));
     }
@@ -1794,6 +1821,9 @@ void batch_impl(const std::vector<BatchItemHost>& items, uint32_t location, cons
     }
     std::vector<uint32_t> rb(nw + 1, 0);
     if (pl.n_esc > 0) rb = read_at<uint32_t>(pl.esc_first, read_at<uint32_t>(pl.esc_pos, wave_row, ar), ar);
+    std::vector<uint32_t> lb(nw + 1, 0);  // long runs of each wave
+    for (uint32_t w = 0; w <= nw; ++w)
+        lb[w] = (uint32_t)(std::lower_bound(pl.h_esc_long.begin(), pl.h_esc_long.end(), rb[w]) - pl.h_esc_long.begin());
 
     // learned: the claim cursors of every item
     OutputView base;
@@ -1888,7 +1918,7 @@ void batch_impl(const std::vector<BatchItemHost>& items, uint32_t location, cons
                     ovk[kind].fail_list = fail_list[kind];
                     PTC_CUDA(cudaMemsetAsync(fail_count[kind], 0, sizeof(uint32_t), st));
                 }
-                if (pl.rowmap) {
+                if (pl.n_map > 0) {
                     ovm.fail_count = map_fail_count;
                     ovm.fail_list = map_fail_list;
                     PTC_CUDA(cudaMemsetAsync(map_fail_count, 0, sizeof(uint32_t), st));
@@ -1910,11 +1940,12 @@ void batch_impl(const std::vector<BatchItemHost>& items, uint32_t location, cons
                     for (int kind = 0; kind < 2; ++kind)
                         launch_parts(kind, op, parts[kind] + pb[kind][w], pb[kind][w + 1] - pb[kind][w], ovk[kind],
                                      pl.work_counter, op.err, dev.num_sms, st);
-                    if (pl.rowmap)
+                    if (pl.n_map > 0)
                         launch_rowmap(learned ? kRowmapClaim : kRowmapExact, op, map_rows + mb[w], mb[w + 1] - mb[w],
                                       nullptr, pl.row_off, ovm, pl.work_counter, dev.num_sms, st);
                     launch_esc_fold(op, ov, pl.esc_run_key, pl.esc_run_start, rb[w], rb[w + 1], pl.esc_colbits,
-                                    pl.esc_rows, pl.esc_first, pl.row_off, pl.esc_sorted, st);
+                                    pl.esc_rows, pl.esc_first, pl.row_off, pl.esc_sorted,
+                                    pl.esc_long + lb[w], lb[w + 1] - lb[w], st);
                 } catch (...) {
                     cudaStreamEndCapture(st, &graph);
                     if (graph) cudaGraphDestroy(graph);
@@ -1956,7 +1987,7 @@ void batch_impl(const std::vector<BatchItemHost>& items, uint32_t location, cons
                         }
                     }
                 }
-                if (pl.rowmap) {  // rows whose claim did not fit their item's budget
+                if (pl.n_map > 0) {  // rows whose claim did not fit their item's budget
                     const uint32_t nfail = read_scalar(map_fail_count, st);
                     if (nfail > 0) {
                         uint32_t* fr = ar.alloc<uint32_t>(nfail);
@@ -2329,7 +2360,8 @@ ptc_status ptc_autotune(const ptc_batch_item* items, uint32_t n, const ptc_optio
             std::vector<uint32_t> values;
         };
         const std::vector<Knob> knobs = {
-            {&ptc_options::large_rows, {PTC_LARGE_ROWS_AUTO, PTC_LARGE_ROWS_PANELS}},
+            {&ptc_options::large_rows, {PTC_LARGE_ROWS_AUTO, PTC_LARGE_ROWS_PANELS, PTC_LARGE_ROWS_BITMAP}},
+            {&ptc_options::bitmap_max_len, {0, 16, 32, 128, 256}},
             {&ptc_options::panel_width, {0, 64, 128, 256, 512, 1024}},
             {&ptc_options::warp_task_max_len, {0, 256, 4096, 16384}},
             {&ptc_options::small_max_products, {0, 64, 256, 512}},
@@ -2340,8 +2372,8 @@ ptc_status ptc_autotune(const ptc_batch_item* items, uint32_t n, const ptc_optio
         for (const Knob& k : knobs) {
             if (k.field == &ptc_options::panel_width && user_panel != 0) continue;  // the caller fixed it
             // panel knobs matter only where the panel kernels run
-            const bool panel_knob = k.field == &ptc_options::panel_width || k.field == &ptc_options::warp_task_max_len;
-            if (panel_knob && n == 1 && opt.large_rows != PTC_LARGE_ROWS_PANELS) continue;
+            // the bitmap length limit matters only when both kernels share the large rows
+            if (k.field == &ptc_options::bitmap_max_len && opt.large_rows != PTC_LARGE_ROWS_AUTO) continue;
             const uint32_t start = opt.*k.field;
             for (uint32_t v : k.values) {
                 if (v == start) continue;

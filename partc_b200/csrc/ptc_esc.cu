@@ -77,14 +77,16 @@ __global__ void esc_gather_kernel(const double* __restrict__ val, const uint32_t
 __global__ void esc_fold_kernel(Operands op, OutputView out, const uint64_t* __restrict__ run_key,
                                 const uint32_t* __restrict__ run_start, uint64_t r0, uint64_t r1, uint32_t colbits,
                                 const uint32_t* __restrict__ esc_rows, const uint32_t* __restrict__ first_run,
-                                const uint64_t* __restrict__ row_off, const double* __restrict__ sorted) {
+                                const uint64_t* __restrict__ row_off, const double* __restrict__ sorted,
+                                uint32_t long_min) {
     const uint64_t r = r0 + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= r1) return;
+    const uint32_t b = run_start[r], en = run_start[r + 1];
+    if (en - b >= long_min) return;  // a long run: esc_fold_long_kernel folds it
     const uint64_t key = run_key[r];
     const uint32_t e = (uint32_t)(key >> colbits);
     const uint32_t row = esc_rows[e];
     const uint32_t col = (uint32_t)(key & ((1ull << colbits) - 1));
-    const uint32_t b = run_start[r], en = run_start[r + 1];
     double v = sorted[b];
     uint32_t i = b + 1;
     constexpr uint32_t U = 16;
@@ -111,6 +113,67 @@ __global__ void esc_fold_kernel(Operands op, OutputView out, const uint64_t* __r
     write_entry(op, out, row_off[row] + (r - first_run[e]), row, col, v);
 }
 
+// One block per long run (runs at least kEscLongMin products long: an output entry that many
+// products meet, e.g. a popular column of a skewed tensor).  The left fold is a chain of
+// dependent additions, so one thread does it -- from shared memory, while warps 1..7 stream the
+// next stage of the run into the other buffer with coalesced loads.
+constexpr int kLongThreads = 256;
+constexpr uint32_t kLongStage = 2048;  // products per stage (16 KiB)
+
+__global__ void __launch_bounds__(kLongThreads)
+    esc_fold_long_kernel(Operands op, OutputView out, const uint64_t* __restrict__ run_key,
+                         const uint32_t* __restrict__ run_start, const uint32_t* __restrict__ long_runs, uint32_t colbits,
+                         const uint32_t* __restrict__ esc_rows, const uint32_t* __restrict__ first_run,
+                         const uint64_t* __restrict__ row_off, const double* __restrict__ sorted) {
+    __shared__ double buf[2][kLongStage];
+    const uint32_t t = threadIdx.x;
+    const uint32_t r = long_runs[blockIdx.x];
+    const uint32_t b = run_start[r], n = run_start[r + 1] - b;
+    const uint32_t nst = (n + kLongStage - 1) / kLongStage;
+    for (uint32_t i = t; i < min(n, kLongStage); i += kLongThreads) buf[0][i] = sorted[b + i];
+    __syncthreads();
+    double v = 0.0;
+    for (uint32_t s = 0; s < nst; ++s) {
+        const uint32_t len = min(kLongStage, n - s * kLongStage);
+        if (t >= 32) {  // warps 1..7 load stage s + 1
+            if (s + 1 < nst) {
+                const uint32_t base = (s + 1) * kLongStage, l2 = min(kLongStage, n - base);
+                double* dst = buf[(s + 1) & 1];
+                for (uint32_t i = t - 32; i < l2; i += kLongThreads - 32) dst[i] = sorted[b + base + i];
+            }
+        } else if (t == 0) {  // the fold, in stream order
+            const double* src = buf[s & 1];
+            uint32_t i = 0;
+            if (s == 0) {
+                v = src[0];
+                i = 1;
+            }
+#pragma unroll 8
+            for (; i < len; ++i) v = __dadd_rn(v, src[i]);
+        }
+        __syncthreads();
+    }
+    if (t == 0) {
+        const uint64_t key = run_key[r];
+        const uint32_t e = (uint32_t)(key >> colbits);
+        const uint32_t row = esc_rows[e];
+        write_entry(op, out, row_off[row] + (r - first_run[e]), row, (uint32_t)(key & ((1ull << colbits) - 1)), v);
+    }
+}
+
+// flag[r] = 1 if run r has at least kEscLongMin products
+__global__ void esc_long_flags_kernel(const uint32_t* __restrict__ run_start, uint64_t nruns, uint32_t* __restrict__ flag) {
+    const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < nruns) flag[r] = (run_start[r + 1] - run_start[r] >= kEscLongMin) ? 1u : 0u;
+}
+
+void launch_esc_long_flags(const uint32_t* run_start, uint64_t nruns, uint32_t* flag, cudaStream_t st) {
+    if (nruns == 0) return;
+    esc_long_flags_kernel<<<ceil_div_u32(nruns, 256), 256, 0, st>>>(run_start, nruns, flag);
+    count_launch();
+    PTC_CHECK_LAUNCH();
+}
+
 void launch_esc_gather(const uint32_t* perm, const double* val, uint64_t nprod, double* sorted, cudaStream_t st) {
     if (nprod == 0) return;
     esc_gather_kernel<<<ceil_div_u32(nprod, 256), 256, 0, st>>>(val, perm, nprod, sorted);
@@ -120,10 +183,18 @@ void launch_esc_gather(const uint32_t* perm, const double* val, uint64_t nprod, 
 
 void launch_esc_fold(const Operands& op, const OutputView& out, const uint64_t* run_key, const uint32_t* run_start,
                      uint64_t r0, uint64_t r1, uint32_t colbits, const uint32_t* esc_rows, const uint32_t* first_run,
-                     const uint64_t* row_off, const double* sorted, cudaStream_t st) {
+                     const uint64_t* row_off, const double* sorted, const uint32_t* long_runs, uint32_t n_long,
+                     cudaStream_t st) {
     if (r1 <= r0) return;
+    if (n_long > 0) {  // the long runs first: each is a long chain, so they start as early as possible
+        esc_fold_long_kernel<<<n_long, kLongThreads, 0, st>>>(op, out, run_key, run_start, long_runs, colbits,
+                                                               esc_rows, first_run, row_off, sorted);
+        count_launch();
+        PTC_CHECK_LAUNCH();
+    }
     esc_fold_kernel<<<ceil_div_u32(r1 - r0, 128), 128, 0, st>>>(op, out, run_key, run_start, r0, r1, colbits,
-                                                                esc_rows, first_run, row_off, sorted);
+                                                                esc_rows, first_run, row_off, sorted,
+                                                                kEscLongMin);
     count_launch();
     PTC_CHECK_LAUNCH();
 }

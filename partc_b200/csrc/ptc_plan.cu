@@ -55,18 +55,20 @@ void launch_compact_indices(const uint32_t* flag, const uint32_t* pos, uint64_t 
 }
 
 __global__ void work_keys_kernel(const uint32_t* __restrict__ rows, uint64_t n, const uint64_t* __restrict__ row_flops,
-                                 const uint32_t* __restrict__ row_start, uint32_t max_len, uint64_t* __restrict__ key) {
+                                 const uint32_t* __restrict__ row_start, uint32_t map_len, uint32_t max_len,
+                                 uint64_t* __restrict__ key) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t r = rows[i];
-    const uint64_t block_row = (row_start[r + 1] - row_start[r]) > max_len ? 1ull : 0ull;
-    key[i] = (block_row << 40) | (~row_flops[r] & ((1ull << 40) - 1));
+    const uint32_t len = row_start[r + 1] - row_start[r];
+    const uint64_t group = len <= map_len ? 0ull : len <= max_len ? 1ull : 2ull;
+    key[i] = (group << 40) | (~row_flops[r] & ((1ull << 40) - 1));
 }
 
 void launch_work_keys(const uint32_t* rows, uint64_t n, const uint64_t* row_flops, const uint32_t* row_start,
-                      uint32_t max_len, uint64_t* key, cudaStream_t st) {
+                      uint32_t map_len, uint32_t max_len, uint64_t* key, cudaStream_t st) {
     if (n == 0) return;
-    work_keys_kernel<<<ceil_div_u32(n, 256), 256, 0, st>>>(rows, n, row_flops, row_start, max_len, key);
+    work_keys_kernel<<<ceil_div_u32(n, 256), 256, 0, st>>>(rows, n, row_flops, row_start, map_len, max_len, key);
     count_launch();
     PTC_CHECK_LAUNCH();
 }

@@ -66,16 +66,26 @@ void launch_esc_count(const uint64_t* run_key, uint64_t nruns, uint32_t colbits,
                       uint64_t* row_d, uint32_t* first_run, cudaStream_t st);
 // sorted[i] = val[perm[i]] for the nprod sorted products
 void launch_esc_gather(const uint32_t* perm, const double* val, uint64_t nprod, double* sorted, cudaStream_t st);
-// runs [r0, r1) of the sorted products: one output entry each
+// runs of at least this many products are folded by a block each (esc_fold_long_kernel)
+constexpr uint32_t kEscLongMin = 16384;
+// flag[r] = 1 for the runs of at least kEscLongMin products
+void launch_esc_long_flags(const uint32_t* run_start, uint64_t nruns, uint32_t* flag, cudaStream_t st);
+// runs [r0, r1) of the sorted products: one output entry each; long_runs[0, n_long) are the long
+// runs among them (the other runs fold one per thread)
 void launch_esc_fold(const Operands& op, const OutputView& out, const uint64_t* run_key, const uint32_t* run_start,
                      uint64_t r0, uint64_t r1, uint32_t colbits, const uint32_t* esc_rows, const uint32_t* first_run,
-                     const uint64_t* row_off, const double* sorted, cudaStream_t st);
+                     const uint64_t* row_off, const double* sorted, const uint32_t* long_runs, uint32_t n_long,
+                     cudaStream_t st);
 // out[pos[i]] = i wherever flag[i] (pos = exclusive scan of flag)
 void launch_compact_indices(const uint32_t* flag, const uint32_t* pos, uint64_t n, uint32_t* out, cudaStream_t st);
-// key[i] = (row has more than max_len A nonzeros) << 40 | ~row_flops[rows[i]] (low 40 bits): sorted,
-// the rows for warp tasks come first, each group largest first
+// key[i] = group << 40 | ~row_flops[rows[i]] (low 40 bits), group 0 for rows of at most map_len
+// A nonzeros (the row bitmap kernel), 1 up to max_len (warp tasks), 2 above (block parts):
+// sorted, the groups come in that order, each largest first
 void launch_work_keys(const uint32_t* rows, uint64_t n, const uint64_t* row_flops, const uint32_t* row_start,
-                      uint32_t max_len, uint64_t* key, cudaStream_t st);
+                      uint32_t map_len, uint32_t max_len, uint64_t* key, cudaStream_t st);
+// rows whose A nonzeros number at most this go to the row bitmap kernel (one barrier round per A
+// nonzero); longer rows to the panel kernels
+constexpr uint32_t kBitmapMaxLen = 64;
 // How a large row is cut into parts, from its exact output count per fine panel: windows of
 // dense_panels panels holding at least dense_min entries per panel become dense parts; the
 // other panels are grouped greedily into open-addressing parts of at most cap entries.
