@@ -582,6 +582,17 @@ struct Launched {
     uint32_t* item_count;
 };
 
+// Exact symbolic pass of large rows for the panel kernels: per-panel counts (panel_cnt, pbase as
+// launch_sym_bitmap takes them) and row totals added to row_d.  One bitmap of each row's columns
+// in shared memory when they fit (launch_row_counts), else the windowed bitmap pass.
+void exact_panel_counts(const Operands& op, const uint32_t* rows, uint32_t n, uint32_t* panel_cnt,
+                        const uint64_t* pbase, uint64_t* row_d, uint32_t* work_counter, int num_sms, cudaStream_t st) {
+    if (op.ncols <= row_counts_max_cols() && op.panel_log2 >= 5)
+        launch_row_counts(op, rows, n, panel_cnt, pbase, row_d, work_counter, num_sms, st);
+    else
+        launch_sym_bitmap(op, rows, n, panel_cnt, pbase, row_d, work_counter, num_sms, st);
+}
+
 // Learned path of a single contraction, after the first numeric pass: work items whose
 // accumulator overflowed or whose claim did not fit wrote nothing and are listed in their launch's
 // fail list.  Their rows get the exact symbolic pass, each failed item is re-split exactly into
@@ -622,7 +633,7 @@ uint64_t learned_reruns(const Operands& op, std::vector<Launched> groups, const 
         uint32_t* cnt = ar.alloc<uint32_t>((uint64_t)nr * P);
         uint64_t* scratch_d = ar.alloc<uint64_t>(nrows);
         PTC_CUDA(cudaMemsetAsync(scratch_d, 0, nrows * sizeof(uint64_t), st));
-        launch_sym_bitmap(op, drows, nr, cnt, nullptr, scratch_d, work_counter, num_sms, st);
+        exact_panel_counts(op, drows, nr, cnt, nullptr, scratch_d, work_counter, num_sms, st);
         uint32_t* np = ar.alloc<uint32_t>((uint64_t)nfail + 1);
         uint32_t* tot = ar.alloc<uint32_t>(nfail);
         launch_count_parts_range(failed, dridx, nfail, cnt, P, rule, np, tot, st);
@@ -852,7 +863,7 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
                 "large_rows = PTC_LARGE_ROWS_BITMAP: at most about 600k distinct B free keys per contraction");
     const uint32_t map_len = !bitmap_ok ? 0u
                              : opt.large_rows == PTC_LARGE_ROWS_BITMAP ? UINT32_MAX
-                             : (opt.bitmap_max_len ? opt.bitmap_max_len : kBitmapMaxLen);
+                             : opt.bitmap_max_len;
     const uint32_t warp_len = (opt.panel_width == 0 || opt.panel_width <= warp_task_dense_columns())
                                   ? (opt.warp_task_max_len ? opt.warp_task_max_len : kWarpTaskMaxLen) : 0u;
     if (n_big > 0) {
@@ -970,8 +981,8 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
     if (!pl.learned) {
         const uint32_t nm = pl.n_mapped;
         launch_rowmap(kRowmapCount, op, pl.big_rows, nm, row_d, nullptr, none, pl.work_counter, num_sms, st);
-        launch_sym_bitmap(op, pl.big_rows + nm, n_big - nm, pbase ? panel_cnt : panel_cnt + (uint64_t)nm * P,
-                          pbase ? pbase + nm : nullptr, row_d, pl.work_counter, num_sms, st);
+        exact_panel_counts(op, pl.big_rows + nm, n_big - nm, pbase ? panel_cnt : panel_cnt + (uint64_t)nm * P,
+                           pbase ? pbase + nm : nullptr, row_d, pl.work_counter, num_sms, st);
     }
     // sort-based rows: expand their products in stream order, sort stably by (row, column)
     pl.esc_colbits = (uint32_t)colbits;
@@ -2361,7 +2372,7 @@ ptc_status ptc_autotune(const ptc_batch_item* items, uint32_t n, const ptc_optio
         };
         const std::vector<Knob> knobs = {
             {&ptc_options::large_rows, {PTC_LARGE_ROWS_AUTO, PTC_LARGE_ROWS_PANELS, PTC_LARGE_ROWS_BITMAP}},
-            {&ptc_options::bitmap_max_len, {0, 16, 32, 128, 256}},
+            {&ptc_options::bitmap_max_len, {0, 8, 32}},
             {&ptc_options::panel_width, {0, 64, 128, 256, 512, 1024}},
             {&ptc_options::warp_task_max_len, {0, 256, 4096, 16384}},
             {&ptc_options::small_max_products, {0, 64, 256, 512}},

@@ -110,8 +110,9 @@ template <int MODE, int FA, int FB>
 __global__ void __launch_bounds__(kRmThreads, 3)
     rowmap_kernel(Operands op, const uint32_t* __restrict__ rows, uint32_t nrows, uint64_t* __restrict__ row_d,
                   const uint64_t* __restrict__ row_off, OutputView out, uint32_t* __restrict__ work_counter,
-                  uint32_t nwords) {
+                  uint32_t nwords, uint32_t* __restrict__ panel_cnt, const uint64_t* __restrict__ pbase) {
     extern __shared__ __align__(16) uint32_t sm[];
+    // the count mode needs the bitmap alone
     uint32_t* bits = sm;                 // [nwords] columns of the row
     uint32_t* wrote = sm + nwords;       // [nwords] columns that hold a value already
     uint32_t* pref = sm + 2 * nwords;    // [nwords] set bits before each word
@@ -123,7 +124,8 @@ __global__ void __launch_bounds__(kRmThreads, 3)
     const uint32_t t = threadIdx.x, lane = lane_id(), warp = t >> 5;
     {
         uint4* b4 = reinterpret_cast<uint4*>(sm);
-        for (uint32_t i = t; i < nwords / 2; i += kRmThreads) b4[i] = make_uint4(0, 0, 0, 0);  // bits, wrote
+        const uint32_t n4 = (MODE == kRowmapCount ? nwords : 2 * nwords) / 4;  // bits (and wrote)
+        for (uint32_t i = t; i < n4; i += kRmThreads) b4[i] = make_uint4(0, 0, 0, 0);
     }
 
     for (;;) {
@@ -167,21 +169,38 @@ __global__ void __launch_bounds__(kRmThreads, 3)
             __syncthreads();
         }
 
-        // B. word prefixes: thread t takes words [t * per, (t + 1) * per)
-        const uint32_t per = (nw + kRmThreads - 1) / kRmThreads;
-        const uint32_t w0 = min(nw, t * per), w1 = min(nw, w0 + per);
-        uint32_t mine = 0;
-        for (uint32_t w = w0; w < w1; ++w) mine += __popc(bits[w]);
-        uint32_t count;
-        uint32_t run = block_exclusive_scan<uint32_t, kRmThreads>(mine, tmp, &count);
-        for (uint32_t w = w0; w < w1; ++w) {
-            pref[w] = run;
-            run += __popc(bits[w]);
-        }
-
         if (MODE == kRowmapCount) {
-            if (t == 0) row_d[row] = count;
+            // the row's output count per fine panel (panels are whole bitmap words: 2^panel_log2
+            // >= 32 columns) when panel_cnt is given, and in total
+            uint32_t mine = 0;
+            if (panel_cnt) {
+                const uint32_t wpp = (1u << op.panel_log2) >> 5;
+                const uint64_t pb = pbase ? pbase[item] : (uint64_t)item * op.npanels;
+                const uint32_t pn = pbase ? (uint32_t)(pbase[item + 1] - pbase[item]) : op.npanels;
+                for (uint32_t p = t; p < pn; p += kRmThreads) {
+                    uint32_t c = 0;
+                    for (uint32_t w = p * wpp; w < min(nw, (p + 1) * wpp); ++w) c += __popc(bits[w]);
+                    panel_cnt[pb + p] = c;
+                    mine += c;
+                }
+            } else {
+                for (uint32_t w = t; w < nw; w += kRmThreads) mine += __popc(bits[w]);
+            }
+            uint32_t count;
+            block_exclusive_scan<uint32_t, kRmThreads>(mine, tmp, &count);
+            if (t == 0) atomicAdd(reinterpret_cast<unsigned long long*>(&row_d[row]), (unsigned long long)count);
         } else {
+            // B. word prefixes: thread t takes words [t * per, (t + 1) * per)
+            const uint32_t per = (nw + kRmThreads - 1) / kRmThreads;
+            const uint32_t w0 = min(nw, t * per), w1 = min(nw, w0 + per);
+            uint32_t mine = 0;
+            for (uint32_t w = w0; w < w1; ++w) mine += __popc(bits[w]);
+            uint32_t count;
+            uint32_t run = block_exclusive_scan<uint32_t, kRmThreads>(mine, tmp, &count);
+            for (uint32_t w = w0; w < w1; ++w) {
+                pref[w] = run;
+                run += __popc(bits[w]);
+            }
             if (t == 0) {
                 uint64_t base = 0;
                 if (MODE == kRowmapExact) {
@@ -298,14 +317,15 @@ __global__ void __launch_bounds__(kRmThreads, 3)
         // clear the row's words for the next row
         for (uint32_t w = t; w < nw; w += kRmThreads) {
             bits[w] = 0;
-            wrote[w] = 0;
+            if (MODE != kRowmapCount) wrote[w] = 0;
         }
     }
 }
 
 template <int MODE>
 void launch_mode(const Operands& op, const uint32_t* rows, uint32_t nrows, uint64_t* row_d, const uint64_t* row_off,
-                 const OutputView& out, uint32_t* work_counter, int num_sms, cudaStream_t st) {
+                 const OutputView& out, uint32_t* work_counter, int num_sms, cudaStream_t st,
+                 uint32_t* panel_cnt = nullptr, const uint64_t* pbase = nullptr) {
     auto kernel = rowmap_kernel<MODE, 0, 0>;
     const bool plain = !out.row_of && !op.row_item;
     if (MODE == kRowmapCount || (plain && op.fa == 2 && op.fb == 2)) kernel = rowmap_kernel<MODE, 2, 2>;
@@ -313,14 +333,15 @@ void launch_mode(const Operands& op, const uint32_t* rows, uint32_t nrows, uint6
     else if (plain && op.fa == 1 && op.fb == 2) kernel = rowmap_kernel<MODE, 1, 2>;
     else if (plain && op.fa == 2 && op.fb == 1) kernel = rowmap_kernel<MODE, 2, 1>;
     const uint32_t nwords = rm_words(op.ncols);
-    const size_t smem = (size_t)3 * nwords * sizeof(uint32_t);
+    const size_t smem = (size_t)(MODE == kRowmapCount ? 1 : 3) * nwords * sizeof(uint32_t);
     PTC_CUDA(cudaMemsetAsync(work_counter, 0, sizeof(uint32_t), st));
     PTC_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 1;
     PTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kRmThreads, smem));
     per_sm = per_sm < 1 ? 1 : per_sm;
     const uint32_t grid = (uint32_t)std::min<uint64_t>(nrows, (uint64_t)num_sms * per_sm);
-    kernel<<<grid, kRmThreads, smem, st>>>(op, rows, nrows, row_d, row_off, out, work_counter, nwords);
+    kernel<<<grid, kRmThreads, smem, st>>>(op, rows, nrows, row_d, row_off, out, work_counter, nwords, panel_cnt,
+                                           pbase);
     count_launch();
     PTC_CHECK_LAUNCH();
 }
@@ -379,6 +400,18 @@ void launch_row_wave(const uint32_t* rows, uint32_t n, const uint32_t* wave_row,
     count_launch();
     PTC_CHECK_LAUNCH();
 }
+
+void launch_row_counts(const Operands& op, const uint32_t* rows, uint32_t nrows, uint32_t* panel_cnt,
+                       const uint64_t* pbase, uint64_t* row_d, uint32_t* work_counter, int num_sms, cudaStream_t st) {
+    if (nrows == 0) return;
+    PTC_REQUIRE(op.ncols <= row_counts_max_cols() && (op.row_item == nullptr || op.item_cols != nullptr) &&
+                    (!panel_cnt || op.panel_log2 >= 5),
+                PTC_ERR_INTERNAL, "bitmap count: too many columns, or panels narrower than a bitmap word");
+    launch_mode<kRowmapCount>(op, rows, nrows, row_d, nullptr, OutputView{}, work_counter, num_sms, st, panel_cnt,
+                              pbase);
+}
+
+uint64_t row_counts_max_cols() { return (uint64_t)(kRmSmemLimit / sizeof(uint32_t)) * 32 - 128; }
 
 uint64_t rowmap_max_cols() {
     // three bitmaps' worth of words (bits, written, prefixes) in one block's shared memory

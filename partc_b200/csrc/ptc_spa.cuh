@@ -83,9 +83,7 @@ void launch_compact_indices(const uint32_t* flag, const uint32_t* pos, uint64_t 
 // sorted, the groups come in that order, each largest first
 void launch_work_keys(const uint32_t* rows, uint64_t n, const uint64_t* row_flops, const uint32_t* row_start,
                       uint32_t map_len, uint32_t max_len, uint64_t* key, cudaStream_t st);
-// rows whose A nonzeros number at most this go to the row bitmap kernel (one barrier round per A
-// nonzero); longer rows to the panel kernels
-constexpr uint32_t kBitmapMaxLen = 64;
+
 // How a large row is cut into parts, from its exact output count per fine panel: windows of
 // dense_panels panels holding at least dense_min entries per panel become dense parts; the
 // other panels are grouped greedily into open-addressing parts of at most cap entries.
