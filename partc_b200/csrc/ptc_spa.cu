@@ -354,6 +354,26 @@ uint32_t warp_task_dense_columns() { return kTaskDense; }
 uint32_t warp_task_min_bits() { return 6; }                   // 64 slots: two per lane
 uint32_t warp_task_max_bits() { return 9; }
 
+// A sub-range of at least this many products is streamed on its own (see warp_task_kernel)
+constexpr uint32_t kStreamMin = 16;
+constexpr int kStreamUnroll = 4;
+
+// Slot of column `col` in an open-addressing table of tmask + 1 = tsize slots (linear probing,
+// inserted with atomicCAS if absent), or -1 when the table is full.
+__device__ __forceinline__ int table_slot(uint32_t* keys, uint32_t col, uint32_t tmask, uint32_t tsize) {
+    uint32_t h = hash32(col) & tmask;
+    for (uint32_t probe = 0; probe < tsize; ++probe) {
+        const uint32_t cv = keys[h];
+        if (cv == col) return (int)h;
+        if (cv == kEmptyCol) {
+            const uint32_t old = atomicCAS(&keys[h], kEmptyCol, col);
+            if (old == kEmptyCol || old == col) return (int)h;
+        }
+        h = (h + 1) & tmask;
+    }
+    return -1;
+}
+
 // One chunk of 32 products of a task: lane l takes product q0 + l of the packed stream.
 struct Chunk {
     uint32_t kk;    // source lane (the A nonzero of this window)
@@ -386,9 +406,12 @@ __device__ __forceinline__ Chunk load_chunk(const Operands& op, uint32_t q0, uin
     return c;
 }
 
+// 32-slot groups a warp emits at a time (their column-tuple loads are in flight together)
+constexpr int kEmitGroups = 4;
+
 // Emit the warp's table: entries in slot order (column order for a dense task) from output
-// position `base`, resetting the table.  Four 32-slot groups at a time, so their tuple loads are
-// in flight together.  fa/fb > 0: the single-contraction layout with those free-mode counts.
+// position `base`, resetting the table.  kEmitGroups 32-slot groups at a time, so their tuple
+// loads are in flight together.  fa/fb > 0: the single-contraction layout with those free-mode counts.
 template <int FA, int FB>
 __device__ __forceinline__ void emit_table(const Operands& op, const OutputView& out, uint64_t base, uint32_t row,
                                            uint32_t c0, bool dense, uint32_t tsize, double* vals, uint32_t* keys) {
@@ -398,13 +421,13 @@ __device__ __forceinline__ void emit_table(const Operands& op, const OutputView&
     if (FA > 0)
         for (int m = 0; m < FA; ++m) rt[m] = op.row_tuple[(uint64_t)row * FA + m];
     uint64_t o = base;
-    for (uint32_t i = 0; i < tsize; i += 128) {
-        bool occ[4];
-        uint32_t col[4];
-        double v[4];
-        uint32_t m[4];
+    for (uint32_t i = 0; i < tsize; i += 32 * kEmitGroups) {
+        bool occ[kEmitGroups];
+        uint32_t col[kEmitGroups];
+        double v[kEmitGroups];
+        uint32_t m[kEmitGroups];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int u = 0; u < kEmitGroups; ++u) {
             const uint32_t sidx = i + u * 32 + lane;
             occ[u] = false;
             if (i + u * 32 < tsize) {
@@ -420,13 +443,13 @@ __device__ __forceinline__ void emit_table(const Operands& op, const OutputView&
         }
         if (base == ~0ull) continue;  // rerun later: nothing written
         if (FA > 0) {
-            uint32_t ct[4][FB > 0 ? FB : 1];
+            uint32_t ct[kEmitGroups][FB > 0 ? FB : 1];
 #pragma unroll
-            for (int u = 0; u < 4; ++u)
+            for (int u = 0; u < kEmitGroups; ++u)
                 if (occ[u])
                     for (int k = 0; k < FB; ++k) ct[u][k] = op.col_tuple[(uint64_t)col[u] * FB + k];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < kEmitGroups; ++u) {
                 if (occ[u]) {
                     const uint64_t e = o + __popc(m[u] & lanemask_lt());
                     uint32_t* dst = out.idx + e * (FA + FB);
@@ -444,7 +467,7 @@ __device__ __forceinline__ void emit_table(const Operands& op, const OutputView&
             }
         } else {
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < kEmitGroups; ++u) {
                 if (occ[u]) write_entry(op, out, o + __popc(m[u] & lanemask_lt()), row, col[u], v[u]);
                 o += __popc(m[u]);
             }
@@ -465,11 +488,14 @@ __global__ void __launch_bounds__(kTaskWarps * 32, kTaskBlocksPerSm)
     bool dense_layout = true;
     __syncwarp();
 
+    // Tasks come from a counter one ahead: lane 0 takes the index of the following task while the
+    // current one starts, so the atomic's latency is off the warp's path.
+    uint32_t tn = 0;
+    if (lane == 0) tn = atomicAdd(work_counter, 1u);
+    uint32_t t = __shfl_sync(kFullMask, tn, 0);
     for (;;) {
-        uint32_t t = 0;
-        if (lane == 0) t = atomicAdd(work_counter, 1u);
-        t = __shfl_sync(kFullMask, t, 0);
         if (t >= ntasks) break;
+        if (lane == 0) tn = atomicAdd(work_counter, 1u);
         const PartItem it = tasks[t];
         const bool dense = (it.mode & 1u) != 0;
         const uint32_t tsize = dense ? kTaskDense : (1u << (it.mode >> 1));
@@ -501,57 +527,94 @@ __global__ void __launch_bounds__(kTaskWarps * 32, kTaskBlocksPerSm)
                     a = op.a_val[k];
                 }
             }
-            const uint32_t incl = warp_inclusive_scan(L);
-            const uint32_t excl = incl - L;
-            const uint32_t total = __shfl_sync(kFullMask, incl, 31);
-            // software pipeline: the next chunk's fiber entries load while this one is applied
-            Chunk nxt = total > 0 ? load_chunk(op, 0, total, incl, s, excl) : Chunk{0u, kEmptyCol, 0.0};
-            for (uint32_t q0 = 0; q0 < total; q0 += 32) {
-                const Chunk cur = nxt;
-                if (q0 + 32 < total) nxt = load_chunk(op, q0 + 32, total, incl, s, excl);
-                const bool valid = cur.col != kEmptyCol;
-                const uint32_t col = cur.col;
-                const double ak = __shfl_sync(kFullMask, a, cur.kk);
-                const double prod = valid ? __dmul_rn(ak, cur.bval) : 0.0;
-                // products of a single A nonzero have distinct columns: no ordering inside the chunk
-                const uint32_t k0 = __shfl_sync(kFullMask, cur.kk, 0);
-                const bool single = __all_sync(kFullMask, !valid || cur.kk == k0);
-                int slot = -1;
-                uint32_t rank = 0;
-                if (dense) {
-                    const uint32_t d = col - c0;
-                    if (valid) {
-                        if (d < kTaskDense) slot = (int)d;
-                        else bad = true;
-                    }
-                    if (!single) rank = __popc(__match_any_sync(kFullMask, slot) & lanemask_lt());
-                } else {
-                    uint32_t leader = lane;
-                    if (!single) {
-                        const uint32_t mm = __match_any_sync(kFullMask, col);
-                        rank = __popc(mm & lanemask_lt());
-                        leader = __ffs(mm) - 1;
-                    }
-                    if (valid && rank == 0) {
-                        uint32_t h = hash32(col) & tmask;
-                        for (uint32_t probe = 0; probe < tsize; ++probe) {
-                            const uint32_t cv = keys[h];
-                            if (cv == col) { slot = (int)h; break; }
-                            if (cv == kEmptyCol) {
-                                const uint32_t old = atomicCAS(&keys[h], kEmptyCol, col);
-                                if (old == kEmptyCol || old == col) { slot = (int)h; break; }
+            // A nonzeros with at least kStreamMin products in the task are streamed one after the
+            // other, 32 lanes over the sub-range, kStreamUnroll entries in flight per lane: the
+            // columns of one sub-range are distinct, so no ordering is needed inside it.  Runs of
+            // shorter sub-ranges between them are packed 32 products per step, in stream order,
+            // and products meeting in one column are applied by rank (match_any).
+            const uint32_t longm = __ballot_sync(kFullMask, L >= kStreamMin);
+            uint32_t lo = 0;
+            while (lo < 32) {
+                const uint32_t m = longm & ~((1u << lo) - 1u);
+                const uint32_t nl = m ? (uint32_t)(__ffs(m) - 1) : 32u;
+                if (nl > lo) {  // lanes [lo, nl): short sub-ranges, packed
+                    const uint32_t Lp = (lane >= lo && lane < nl) ? L : 0u;
+                    const uint32_t incl = warp_inclusive_scan(Lp);
+                    const uint32_t excl = incl - Lp;
+                    const uint32_t total = __shfl_sync(kFullMask, incl, 31);
+                    // software pipeline: the next chunk's fiber entries load while this one is applied
+                    Chunk nxt = total > 0 ? load_chunk(op, 0, total, incl, s, excl) : Chunk{0u, kEmptyCol, 0.0};
+                    for (uint32_t q0 = 0; q0 < total; q0 += 32) {
+                        const Chunk cur = nxt;
+                        if (q0 + 32 < total) nxt = load_chunk(op, q0 + 32, total, incl, s, excl);
+                        const bool valid = cur.col != kEmptyCol;
+                        const uint32_t col = cur.col;
+                        const double ak = __shfl_sync(kFullMask, a, cur.kk);
+                        const double prod = valid ? __dmul_rn(ak, cur.bval) : 0.0;
+                        // products of a single A nonzero have distinct columns: no ordering inside
+                        const uint32_t k0 = __shfl_sync(kFullMask, cur.kk, 0);
+                        const bool single = __all_sync(kFullMask, !valid || cur.kk == k0);
+                        int slot = -1;
+                        uint32_t rank = 0;
+                        if (dense) {
+                            const uint32_t d = col - c0;
+                            if (valid) {
+                                if (d < kTaskDense) slot = (int)d;
+                                else bad = true;
                             }
-                            h = (h + 1) & tmask;
+                            if (!single) rank = __popc(__match_any_sync(kFullMask, slot) & lanemask_lt());
+                        } else {
+                            uint32_t leader = lane;
+                            if (!single) {
+                                const uint32_t mm = __match_any_sync(kFullMask, col);
+                                rank = __popc(mm & lanemask_lt());
+                                leader = __ffs(mm) - 1;
+                            }
+                            if (valid && rank == 0) {
+                                slot = table_slot(keys, col, tmask, tsize);
+                                if (slot < 0) bad = true;
+                            }
+                            if (!single) slot = __shfl_sync(kFullMask, slot, leader);
+                        }
+                        const uint32_t maxr = single ? 0u : __reduce_max_sync(kFullMask, valid ? rank : 0u);
+                        for (uint32_t r = 0; r <= maxr; ++r) {
+                            if (valid && rank == r && slot >= 0) accumulate(&vals[slot], prod);
+                            __syncwarp();
+                        }
+                    }
+                }
+                if (nl == 32) break;
+                // lane nl: a long sub-range, streamed
+                const uint32_t sk = __shfl_sync(kFullMask, s, nl), Lk = __shfl_sync(kFullMask, L, nl);
+                const double ak = __shfl_sync(kFullMask, a, nl);
+                for (uint32_t j0 = 0; j0 < Lk; j0 += 32 * kStreamUnroll) {
+                    uint32_t cc[kStreamUnroll];
+                    double bv[kStreamUnroll];
+#pragma unroll
+                    for (int u = 0; u < kStreamUnroll; ++u) {
+                        const uint32_t j = j0 + u * 32 + lane;
+                        cc[u] = kEmptyCol;
+                        if (j < Lk) {
+                            cc[u] = __ldg(op.b_col + sk + j);
+                            bv[u] = __ldg(op.b_val + sk + j);
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < kStreamUnroll; ++u) {
+                        if (cc[u] == kEmptyCol) continue;
+                        int slot;
+                        if (dense) {
+                            const uint32_t d = cc[u] - c0;
+                            slot = d < kTaskDense ? (int)d : -1;
+                        } else {
+                            slot = table_slot(keys, cc[u], tmask, tsize);
                         }
                         if (slot < 0) bad = true;
+                        else accumulate(&vals[slot], __dmul_rn(ak, bv[u]));
                     }
-                    if (!single) slot = __shfl_sync(kFullMask, slot, leader);
                 }
-                const uint32_t maxr = single ? 0u : __reduce_max_sync(kFullMask, valid ? rank : 0u);
-                for (uint32_t r = 0; r <= maxr; ++r) {
-                    if (valid && rank == r && slot >= 0) accumulate(&vals[slot], prod);
-                    __syncwarp();
-                }
+                __syncwarp();  // the next A nonzero sees this one's values
+                lo = nl + 1;
             }
         }
 
@@ -578,6 +641,7 @@ __global__ void __launch_bounds__(kTaskWarps * 32, kTaskBlocksPerSm)
         if (out.item_count && lane == 0) out.item_count[t] = base == ~0ull ? 0u : cnt;
         emit_table<FA, FB>(op, out, base, row, c0, dense, tsize, vals, keys);
         __syncwarp();
+        t = __shfl_sync(kFullMask, tn, 0);
     }
 }
 

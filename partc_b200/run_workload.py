@@ -22,6 +22,8 @@ def main(argv=None):
     ap.add_argument("--large-rows", default="auto", choices=["auto", "bitmap", "panels"])
     ap.add_argument("--bitmap-max-len", type=int, default=0)
     ap.add_argument("--panel-width", type=int, default=0)
+    ap.add_argument("--warp-task-max-len", type=int, default=0)
+    ap.add_argument("--hash-load-pct", type=int, default=0)
     a = ap.parse_args(argv)
     import torch
     from partc_b200 import _lib, gen
@@ -33,7 +35,8 @@ def main(argv=None):
     coo = _lib.device_coo(di.data_ptr(), dv.data_ptr(), t.nnz, t.dims, keep)
     s = torch.cuda.Stream()
     opts = dict(output_location="device", device=torch.cuda.current_device(), stream=s.cuda_stream, path=a.path,
-                large_rows=a.large_rows, bitmap_max_len=a.bitmap_max_len, panel_width=a.panel_width)
+                large_rows=a.large_rows, bitmap_max_len=a.bitmap_max_len, panel_width=a.panel_width,
+                warp_task_max_len=a.warp_task_max_len, hash_load_pct=a.hash_load_pct)
     keys = ("t_build_ms", "t_symbolic_ms", "t_numeric_ms", "t_total_ms", "out_nnz", "mult_adds", "rerun_rows",
             "sizer_mean_abs_log2_err", "rows_hash", "hash_parts", "panel_width", "kernel_launches")
     for _ in range(a.reps):
