@@ -113,51 +113,123 @@ __global__ void esc_fold_kernel(Operands op, OutputView out, const uint64_t* __r
     write_entry(op, out, row_off[row] + (r - first_run[e]), row, col, v);
 }
 
-// One block per long run (runs at least kEscLongMin products long: an output entry that many
-// products meet, e.g. a popular column of a skewed tensor).  The left fold is a chain of
-// dependent additions, so one thread does it -- from shared memory, while warps 1..7 stream the
-// next stage of the run into the other buffer with coalesced loads.
-constexpr int kLongThreads = 256;
-constexpr uint32_t kLongStage = 2048;  // products per stage (16 KiB)
+// One block per long run (runs of at least kEscLongMin products: an output entry that many
+// products meet, e.g. a popular column of a skewed tensor), folded exactly as the left fold but
+// mostly in parallel.  While the running value v stays inside one binade [2^E, 2^(E+1)) (either
+// sign), every double there is an integer multiple of u = 2^(E-52), so the IEEE sum
+// fl(v + x) = v + u * rint(x / u) whenever x / u is not halfway between integers and the exact
+// sum stays strictly inside the binade (at least one step from either end): then the rounded sum
+// is the nearest multiple of u and no tie is broken.  So a tile of 8192 products becomes integer
+// increments k = rint(x / u) (in parallel), a block-wide prefix of them, and the running value
+// (v / u) + prefix is exact up to the first product that breaks a condition -- a tie, a value
+// too large, or a prefix that reaches the binade's ends; that one is added for real
+// (__dadd_rn) and the scan resumes after it with the new binade.  A tile that stops more than
+// kGridMaxStops times (a sum hovering near zero crosses binades all the time), or a running value
+// that is zero, subnormal or not finite, is folded by one thread, product after product.  The
+// result is the sequential left fold to the bit.
+constexpr int kGridThreads = 1024;
+constexpr int kGridPer = 8;                             // products per thread per pass
+constexpr uint32_t kGridTile = kGridThreads * kGridPer; // 8192 products (64 KiB of shared memory)
+constexpr int kGridMaxStops = 8;
 
-__global__ void __launch_bounds__(kLongThreads)
+__global__ void __launch_bounds__(kGridThreads)
     esc_fold_long_kernel(Operands op, OutputView out, const uint64_t* __restrict__ run_key,
                          const uint32_t* __restrict__ run_start, const uint32_t* __restrict__ long_runs, uint32_t colbits,
                          const uint32_t* __restrict__ esc_rows, const uint32_t* __restrict__ first_run,
                          const uint64_t* __restrict__ row_off, const double* __restrict__ sorted) {
-    __shared__ double buf[2][kLongStage];
+    extern __shared__ double tile[];  // [kGridTile]
+    __shared__ unsigned long long scan_tmp[kGridThreads / 32 + 1];
+    __shared__ uint32_t s_first;
+    __shared__ double s_v;
     const uint32_t t = threadIdx.x;
     const uint32_t r = long_runs[blockIdx.x];
     const uint32_t b = run_start[r], n = run_start[r + 1] - b;
-    const uint32_t nst = (n + kLongStage - 1) / kLongStage;
-    for (uint32_t i = t; i < min(n, kLongStage); i += kLongThreads) buf[0][i] = sorted[b + i];
-    __syncthreads();
-    double v = 0.0;
-    for (uint32_t s = 0; s < nst; ++s) {
-        const uint32_t len = min(kLongStage, n - s * kLongStage);
-        if (t >= 32) {  // warps 1..7 load stage s + 1
-            if (s + 1 < nst) {
-                const uint32_t base = (s + 1) * kLongStage, l2 = min(kLongStage, n - base);
-                double* dst = buf[(s + 1) & 1];
-                for (uint32_t i = t - 32; i < l2; i += kLongThreads - 32) dst[i] = sorted[b + base + i];
-            }
-        } else if (t == 0) {  // the fold, in stream order
-            const double* src = buf[s & 1];
-            uint32_t i = 0;
-            if (s == 0) {
-                v = src[0];
-                i = 1;
-            }
-#pragma unroll 8
-            for (; i < len; ++i) v = __dadd_rn(v, src[i]);
-        }
+    if (t == 0) s_v = sorted[b];  // the first product of the entry is its value so far
+    for (uint32_t t0 = 1; t0 < n; t0 += kGridTile) {
+        const uint32_t len = min(kGridTile, n - t0);
+        __syncthreads();  // the previous tile is done with `tile`
+        for (uint32_t e = t; e < len; e += kGridThreads) tile[e] = sorted[b + t0 + e];
         __syncthreads();
+        uint32_t st = 0;  // products of the tile already in s_v
+        for (int stops = 0; st < len; ++stops) {
+            const double v = s_v;
+            const double av = fabs(v);
+            if (stops > kGridMaxStops || !(av >= 2.2250738585072014e-308) || av == INFINITY || v != v) {
+                if (t == 0) {  // one thread, product after product
+                    double w = v;
+                    for (uint32_t e = st; e < len; ++e) w = __dadd_rn(w, tile[e]);
+                    s_v = w;
+                }
+                __syncthreads();
+                break;
+            }
+            int E;
+            frexp(av, &E);
+            --E;                                                  // v in [2^E, 2^(E+1))
+            const double u = ldexp(1.0, E - 52);
+            const long long N = (long long)(v / u);               // exact: |N| in [2^52, 2^53)
+            const long long lo = (1ll << 52), hi = (1ll << 53) - 1;
+            // this thread's products st + t * kGridPer + q, q < kGridPer
+            const uint32_t e0 = st + t * kGridPer;
+            unsigned long long k[kGridPer];
+            bool bad[kGridPer];
+            unsigned long long mine = 0;
+#pragma unroll
+            for (int q = 0; q < kGridPer; ++q) {
+                const uint32_t e = e0 + q;
+                k[q] = 0;
+                bad[q] = false;
+                if (e < len) {
+                    const double x = scalbn(tile[e], 52 - E);     // exact scaling by a power of two
+                    const double ax = fabs(x);
+                    if (!(ax < 9007199254740992.0) || fabs(x - trunc(x)) == 0.5) {
+                        bad[q] = true;                            // too large, not finite, or a tie
+                    } else {
+                        k[q] = (unsigned long long)llrint(x);
+                    }
+                    mine += k[q];
+                }
+            }
+            unsigned long long total;
+            const unsigned long long before = block_exclusive_scan<unsigned long long, kGridThreads>(mine, scan_tmp, &total);
+            // first product whose step is not on the grid
+            uint32_t first = 0xffffffffu;
+            unsigned long long run = (unsigned long long)N + before;
+#pragma unroll
+            for (int q = 0; q < kGridPer; ++q) {
+                const uint32_t e = e0 + q;
+                if (e < len && first == 0xffffffffu) {
+                    run += k[q];
+                    const long long m = (long long)run * (N > 0 ? 1 : -1);
+                    if (bad[q] || !(m > lo && m < hi)) first = e;
+                }
+            }
+            if (t == 0) s_first = 0xffffffffu;
+            __syncthreads();
+            if (first != 0xffffffffu) atomicMin(&s_first, first);
+            __syncthreads();
+            const uint32_t f = s_first;
+            if (f == 0xffffffffu) {  // the whole rest of the tile is on the grid
+                if (t == 0) s_v = (double)(long long)((unsigned long long)N + total) * u;
+                __syncthreads();
+                break;
+            }
+            if (first == f) {  // this thread owns product f: the value before it, then f for real
+                unsigned long long p = (unsigned long long)N + before;
+                for (uint32_t e = e0; e < f; ++e) p += k[e - e0];
+                const double prev = f > st ? (double)(long long)p * u : v;
+                s_v = __dadd_rn(prev, tile[f]);
+            }
+            __syncthreads();
+            st = f + 1;
+        }
     }
+    __syncthreads();
     if (t == 0) {
         const uint64_t key = run_key[r];
         const uint32_t e = (uint32_t)(key >> colbits);
         const uint32_t row = esc_rows[e];
-        write_entry(op, out, row_off[row] + (r - first_run[e]), row, (uint32_t)(key & ((1ull << colbits) - 1)), v);
+        write_entry(op, out, row_off[row] + (r - first_run[e]), row, (uint32_t)(key & ((1ull << colbits) - 1)), s_v);
     }
 }
 
@@ -187,8 +259,10 @@ void launch_esc_fold(const Operands& op, const OutputView& out, const uint64_t* 
                      cudaStream_t st) {
     if (r1 <= r0) return;
     if (n_long > 0) {  // the long runs first: each is a long chain, so they start as early as possible
-        esc_fold_long_kernel<<<n_long, kLongThreads, 0, st>>>(op, out, run_key, run_start, long_runs, colbits,
-                                                               esc_rows, first_run, row_off, sorted);
+        const size_t smem = kGridTile * sizeof(double);
+        PTC_CUDA(cudaFuncSetAttribute(esc_fold_long_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        esc_fold_long_kernel<<<n_long, kGridThreads, smem, st>>>(op, out, run_key, run_start, long_runs, colbits,
+                                                                 esc_rows, first_run, row_off, sorted);
         count_launch();
         PTC_CHECK_LAUNCH();
     }

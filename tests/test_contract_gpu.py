@@ -91,6 +91,45 @@ def test_more_than_two_million_columns(engine, oracle_mod, path):
     assert_same_output(idx, vals, o["idx"], o["vals"], bit_exact=True)
 
 
+def _one_entry_contraction(products):
+    """A (K x 1) times B (K x 1) over mode 0 with b = 1: one output entry whose products are
+    `products` in this order (the left fold's order: A's COO order)."""
+    K = len(products)
+    A = gen.CooTensor(idx=np.stack([np.arange(K), np.zeros(K, np.int64)], 1).astype(np.uint32),
+                      vals=np.asarray(products, np.float64), dims=np.array([K, 1], np.uint32))
+    B = gen.CooTensor(idx=np.stack([np.arange(K), np.zeros(K, np.int64)], 1).astype(np.uint32),
+                      vals=np.ones(K), dims=np.array([K, 1], np.uint32))
+    return A, B
+
+
+@pytest.mark.parametrize("kind", ["squares", "signs", "magnitudes", "ties", "cancel"])
+def test_long_runs_fold_exactly(engine, oracle_mod, kind):
+    """An output entry that 100k+ products meet is folded by a block on the grid of the running
+    value's ulp; the result must still be the sequential left fold to the bit, whatever the
+    values: ties broken by parity, binade crossings, cancellation, magnitudes far apart."""
+    rng = np.random.default_rng(61)
+    n = 120_000
+    if kind == "squares":
+        p = rng.standard_normal(n) ** 2
+    elif kind == "signs":
+        p = rng.standard_normal(n)
+    elif kind == "magnitudes":
+        p = rng.standard_normal(n) * np.exp(rng.uniform(-40, 40, n))
+    elif kind == "ties":
+        p = np.concatenate([[1.0], np.tile([2.0 ** -53, 3 * 2.0 ** -53, 2.0 ** -52, 5 * 2.0 ** -54], n // 4),
+                            rng.random(1000)])
+    else:
+        p = np.tile([1e16, 1.0, -1e16, 3.0, 0.5, -0.25], n // 6).astype(np.float64)
+    A, B = _one_entry_contraction(p)
+    o = oracle_mod.contract(A, B, 1, [0, 1], [0, 1])
+    idx, vals, st = engine.contract(A, B, 1, [0, 1], [0, 1])
+    assert st["out_nnz"] == 1 and o["nnz"] == 1
+    seq = p[0]
+    for x in p[1:].tolist():
+        seq = seq + x
+    assert vals.view(np.uint64)[0] == np.float64(seq).view(np.uint64) == o["vals"].view(np.uint64)[0]
+
+
 def test_output_is_canonical_for_panel_rows(engine, oracle_mod):
     """Rows come out in increasing free-key order; panel rows in increasing column order."""
     t = gen.random_coo([50, 40, 3000], 100_000, [None, None, 1.0], 33, "uniform01")
