@@ -476,6 +476,9 @@ void print_reference_lines(const ptc_stats& s) {
 
 // the learned path sizes accumulators and the output for this many times the predicted count
 constexpr float kSizerMargin = 1.25f;
+// a batch item's budget is the sum over its few large rows, whose relative errors average out
+// less than over a whole contraction's: a wider margin keeps its claims from running short
+constexpr float kSizerBatchMargin = 1.5f;
 
 const SizerHost* sizer_host(const ptc_sizer* s) { return s ? &s->host : nullptr; }
 
@@ -1080,7 +1083,8 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
             pl.pred = ar.alloc<float>(n_big);
             sizer_predict_device(*sizer, fx, n_big, pl.pred, ar);
             launch_predicted_panel_counts(pl.big_rows, n_big, pl.row_flops, pl.pred, gp, op.row_item, item_cols,
-                                          pbase, P, pl.log2w, ncols, kSizerMargin, panel_cnt, ar,
+                                          pbase, P, pl.log2w, ncols, F.batch ? kSizerBatchMargin : kSizerMargin,
+                                          panel_cnt, ar,
                                           F.batch ? &is : nullptr);
             launch_claim_budgets(pl.big_rows, n_big, panel_cnt, pbase, P, pl.claim_off, st);
         }
