@@ -112,6 +112,39 @@ struct Events {
 
 enum { EV_START = 0, EV_H2D, EV_BSIDE, EV_ASIDE, EV_SYM, EV_NUM, EV_D2H, EV_WAVE0, EV_WAVE1 };
 
+// Two more streams per device and host thread for kernels of one call that do not depend on each
+// other (they write disjoint output ranges): fork() orders them after the call's stream so far,
+// join() orders the call's stream after them.
+struct AuxStreams {
+    cudaStream_t s[2] = {nullptr, nullptr};
+    cudaEvent_t fork_ev = nullptr, join_ev[2] = {nullptr, nullptr};
+    void fork(cudaStream_t main) {
+        PTC_CUDA(cudaEventRecord(fork_ev, main));
+        for (cudaStream_t a : s) PTC_CUDA(cudaStreamWaitEvent(a, fork_ev, 0));
+    }
+    void join(cudaStream_t main) {
+        for (int i = 0; i < 2; ++i) {
+            PTC_CUDA(cudaEventRecord(join_ev[i], s[i]));
+            PTC_CUDA(cudaStreamWaitEvent(main, join_ev[i], 0));
+        }
+    }
+};
+
+AuxStreams& aux_streams(int device) {
+    constexpr int kMaxDevices = 64;
+    PTC_REQUIRE(device >= 0 && device < kMaxDevices, PTC_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+    thread_local AuxStreams aux[kMaxDevices];
+    AuxStreams& a = aux[device];
+    if (!a.s[0]) {
+        for (int i = 0; i < 2; ++i) {
+            PTC_CUDA(cudaStreamCreateWithFlags(&a.s[i], cudaStreamNonBlocking));
+            PTC_CUDA(cudaEventCreateWithFlags(&a.join_ev[i], cudaEventDisableTiming));
+        }
+        PTC_CUDA(cudaEventCreateWithFlags(&a.fork_ev, cudaEventDisableTiming));
+    }
+    return a;
+}
+
 // One non-blocking stream per device and host thread, kept for the thread's lifetime.
 cudaStream_t default_stream_for_thread(int device) {
     constexpr int kMaxDevices = 64;
@@ -776,6 +809,7 @@ struct Plan {
     PartItem* parts[2] = {nullptr, nullptr};
     uint32_t n_parts[2] = {0, 0};
     uint32_t* work_counter = nullptr;
+    uint32_t* work_counter2 = nullptr;  // the block parts' counter (they can run beside the warp tasks)
     // collision-free large rows (two-phase path): written product by product, in row order
     uint64_t* alen = nullptr;        // exclusive scan of the A nonzeros' fiber lengths
     uint32_t* copy_rows = nullptr;
@@ -979,6 +1013,7 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
     }
     uint32_t* panel_cnt = ar.alloc<uint32_t>(std::max<uint64_t>(n_panel_cnt, 1));
     pl.work_counter = ar.alloc<uint32_t>(1);
+    pl.work_counter2 = ar.alloc<uint32_t>(1);
     OutputView none;
     launch_small_rows(false, op, pl.small_rows, n_small, row_d, nullptr, none, st);
     if (!pl.learned) {
@@ -1317,21 +1352,28 @@ void contract_impl(const ptc_coo* A, const ptc_coo* Bin, uint32_t c, const uint3
             launch_rowmap(learned ? kRowmapClaim : kRowmapExact, op, pl.map_rows, pl.n_map, nullptr, pl.row_off, mo,
                           pl.work_counter, dev.num_sms, st);
         }
+        OutputView ok[2] = {ov, ov};
         for (int kind = 0; kind < 2; ++kind) {
-            OutputView o = ov;
             if (learned) {
                 const uint32_t n = std::max<uint32_t>(pl.n_parts[kind], 1);
-                o.fail_count = ar.alloc<uint32_t>(1);
-                o.fail_list = ar.alloc<uint32_t>(n);
-                o.item_count = ar.alloc<uint32_t>(n);
-                PTC_CUDA(cudaMemsetAsync(o.fail_count, 0, sizeof(uint32_t), st));
-                groups.push_back({kind, pl.parts[kind], pl.n_parts[kind], o.fail_list, o.fail_count, o.item_count});
+                ok[kind].fail_count = ar.alloc<uint32_t>(1);
+                ok[kind].fail_list = ar.alloc<uint32_t>(n);
+                ok[kind].item_count = ar.alloc<uint32_t>(n);
+                PTC_CUDA(cudaMemsetAsync(ok[kind].fail_count, 0, sizeof(uint32_t), st));
+                groups.push_back({kind, pl.parts[kind], pl.n_parts[kind], ok[kind].fail_list, ok[kind].fail_count,
+                                  ok[kind].item_count});
             }
-            launch_parts(kind, op, pl.parts[kind], pl.n_parts[kind], o, pl.work_counter, op.err, dev.num_sms, st);
         }
+        // the block parts (a tail of a few heavy rows) and the sort-based folds run beside the warp
+        // tasks: they write disjoint output ranges
+        AuxStreams& aux = aux_streams(dev.device);
+        aux.fork(st);
+        launch_parts(1, op, pl.parts[1], pl.n_parts[1], ok[1], pl.work_counter2, op.err, dev.num_sms, aux.s[0]);
         launch_esc_fold(op, ov, pl.esc_run_key, pl.esc_run_start, 0, pl.esc_runs, pl.esc_colbits, pl.esc_rows,
                         pl.esc_first, pl.row_off, pl.esc_sorted, pl.esc_long,
-                        (uint32_t)pl.h_esc_long.size(), st);
+                        (uint32_t)pl.h_esc_long.size(), aux.s[1]);
+        launch_parts(0, op, pl.parts[0], pl.n_parts[0], ok[0], pl.work_counter, op.err, dev.num_sms, st);
+        aux.join(st);
         if (learned) {
             // rows whose prediction fell short run again exactly (parts first, then the bitmap
             // kernel's rows; each grows the output as needed), and the sizer's error over the large
