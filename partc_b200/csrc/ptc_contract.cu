@@ -1988,22 +1988,36 @@ void batch_impl(const std::vector<BatchItemHost>& items, uint32_t location, cons
             cudaGraph_t graph = nullptr;
             cudaGraphExec_t exec = nullptr;
             if (work) {
+                AuxStreams& aux = aux_streams(dev.device);
+                bool forked = false;
                 PTC_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
                 try {
                     launch_small_rows(true, op, pl.small_rows + sb[w], sb[w + 1] - sb[w], nullptr, pl.row_off, ov,
                                       st);
                     launch_copy_rows(op, pl.copy_rows + cb[w], cb[w + 1] - cb[w], pl.alen, pl.row_off, ov,
                                      dev.num_sms, st);
-                    for (int kind = 0; kind < 2; ++kind)
-                        launch_parts(kind, op, parts[kind] + pb[kind][w], pb[kind][w + 1] - pb[kind][w], ovk[kind],
-                                     pl.work_counter, op.err, dev.num_sms, st);
+                    // the block parts and the sort-based folds beside the warp tasks (disjoint
+                    // outputs): branches of the wave's graph
+                    aux.fork(st);
+                    forked = true;
+                    launch_parts(1, op, parts[1] + pb[1][w], pb[1][w + 1] - pb[1][w], ovk[1], pl.work_counter2,
+                                 op.err, dev.num_sms, aux.s[0]);
+                    launch_esc_fold(op, ov, pl.esc_run_key, pl.esc_run_start, rb[w], rb[w + 1], pl.esc_colbits,
+                                    pl.esc_rows, pl.esc_first, pl.row_off, pl.esc_sorted,
+                                    pl.esc_long + lb[w], lb[w + 1] - lb[w], aux.s[1]);
+                    launch_parts(0, op, parts[0] + pb[0][w], pb[0][w + 1] - pb[0][w], ovk[0], pl.work_counter,
+                                 op.err, dev.num_sms, st);
                     if (pl.n_map > 0)
                         launch_rowmap(learned ? kRowmapClaim : kRowmapExact, op, map_rows + mb[w], mb[w + 1] - mb[w],
                                       nullptr, pl.row_off, ovm, pl.work_counter, dev.num_sms, st);
-                    launch_esc_fold(op, ov, pl.esc_run_key, pl.esc_run_start, rb[w], rb[w + 1], pl.esc_colbits,
-                                    pl.esc_rows, pl.esc_first, pl.row_off, pl.esc_sorted,
-                                    pl.esc_long + lb[w], lb[w + 1] - lb[w], st);
+                    aux.join(st);
+                    forked = false;
                 } catch (...) {
+                    if (forked)  // rejoin the branches so the capture can end
+                        for (int i = 0; i < 2; ++i) {
+                            cudaEventRecord(aux.join_ev[i], aux.s[i]);
+                            cudaStreamWaitEvent(st, aux.join_ev[i], 0);
+                        }
                     cudaStreamEndCapture(st, &graph);
                     if (graph) cudaGraphDestroy(graph);
                     throw;
