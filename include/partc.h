@@ -104,7 +104,7 @@ typedef struct ptc_options {
     uint32_t batch_wave_mib;        /* ptc_batch_contract: device memory for one wave's outputs,
                                        MiB (default: 60% of the free memory) */
     uint32_t warp_task_max_len;     /* large rows with at most this many A nonzeros use one warp per
-                                       column range, longer ones one block per part (default 1024) */
+                                       column range, longer ones one block per part (default 256) */
     /* cuckoo build of B's fiber table (the reference's buildHashTable, fksCuckoo.hpp:1044-1060) */
     uint32_t cuckoo_max_chain;      /* evictions one insertion may cause before the build attempt
                                        fails (default 64; 0 = no eviction at all) -- set it small to

@@ -2434,7 +2434,7 @@ ptc_status ptc_autotune(const ptc_batch_item* items, uint32_t n, const ptc_optio
             {&ptc_options::large_rows, {PTC_LARGE_ROWS_AUTO, PTC_LARGE_ROWS_PANELS, PTC_LARGE_ROWS_BITMAP}},
             {&ptc_options::bitmap_max_len, {0, 8, 32}},
             {&ptc_options::panel_width, {0, 64, 128, 256, 512, 1024}},
-            {&ptc_options::warp_task_max_len, {0, 256, 4096, 16384}},
+            {&ptc_options::warp_task_max_len, {0, 64, 1024, 4096}},
             {&ptc_options::small_max_products, {0, 64, 256, 512}},
             {&ptc_options::sort_max_avg_products, {0, 16, 32, 128}},
             {&ptc_options::hash_load_pct, {0, 50, 90}},

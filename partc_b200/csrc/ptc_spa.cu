@@ -34,9 +34,12 @@ __device__ __forceinline__ uint32_t hash32(uint32_t x) {
 // finite or NaN operands can produce (device arithmetic returns the canonical NaN)
 constexpr unsigned long long kNoValue = 0x7ff4deadbeef0001ull;
 
-__device__ __forceinline__ void accumulate(double* slot, double p) {
+// applies product p to a slot; true when the slot held no value before
+__device__ __forceinline__ bool accumulate(double* slot, double p) {
     const double v = *slot;
-    *slot = (__double_as_longlong(v) == (long long)kNoValue) ? p : __dadd_rn(v, p);
+    const bool first = __double_as_longlong(v) == (long long)kNoValue;
+    *slot = first ? p : __dadd_rn(v, p);
+    return first;
 }
 
 // first entry of [lo, hi) (a fiber, sorted by column) whose column is >= c
@@ -344,9 +347,15 @@ constexpr int kTaskWarps = 4;                               // warps per block
 constexpr int kTaskBlocksPerSm = 8;                         // 32 resident warps per SM
 constexpr uint32_t kTaskDense = 768;                        // columns of a dense task
 constexpr uint32_t kTaskSlots = 512;                        // largest sparse table
-constexpr size_t kTaskBytes = kTaskDense * sizeof(double);  // shared memory per warp (6 KiB)
+constexpr size_t kTaskBytes = kTaskDense * sizeof(double);  // a warp's table (6 KiB)
 // the sparse layout keeps values in vals[0, 512) and keys in the bytes of vals[512, 768)
 static_assert(kTaskSlots * (sizeof(double) + sizeof(uint32_t)) <= kTaskBytes, "sparse layout fits a warp's region");
+// Behind the table, the slots a task filled, in the order they were first written: the emission
+// and the claim count visit those alone instead of every slot.  A task that fills more slots
+// than the list holds is emitted by scanning the table.
+constexpr uint32_t kListCap = 384;
+constexpr size_t kWarpBytes = kTaskBytes + kListCap * sizeof(uint16_t);  // 6912 B: 8 blocks of 4 warps per SM
+static_assert(kWarpBytes % 16 == 0, "every warp's region starts 16-byte aligned");
 
 // load factor <= 0.5: linear probes stay short, and a warp waits for its longest one
 uint32_t warp_task_capacity() { return kTaskSlots / 2; }
@@ -406,73 +415,111 @@ __device__ __forceinline__ Chunk load_chunk(const Operands& op, uint32_t q0, uin
     return c;
 }
 
-// 32-slot groups a warp emits at a time (their column-tuple loads are in flight together)
-constexpr int kEmitGroups = 4;
+// 32-entry groups a warp emits at a time (their column-tuple loads are in flight together)
+constexpr int kEmitGroups = 2;
 
-// Emit the warp's table: entries in slot order (column order for a dense task) from output
-// position `base`, resetting the table.  kEmitGroups 32-slot groups at a time, so their tuple
-// loads are in flight together.  fa/fb > 0: the single-contraction layout with those free-mode counts.
+// The single-contraction output layout with fa = FA, fb = FB free modes: the column's index tuple,
+// and output entry e written as row tuple rt (loaded once per task), column tuple ct and value v.
 template <int FA, int FB>
-__device__ __forceinline__ void emit_table(const Operands& op, const OutputView& out, uint64_t base, uint32_t row,
-                                           uint32_t c0, bool dense, uint32_t tsize, double* vals, uint32_t* keys) {
+__device__ __forceinline__ void load_col_tuple(const Operands& op, uint32_t col, uint32_t (&ct)[FB > 0 ? FB : 1]) {
+    if constexpr (FB == 2) {
+        const uint2 c = *reinterpret_cast<const uint2*>(op.col_tuple + (uint64_t)col * 2);
+        ct[0] = c.x;
+        ct[1] = c.y;
+    } else {
+        for (int k = 0; k < FB; ++k) ct[k] = op.col_tuple[(uint64_t)col * FB + k];
+    }
+}
+
+template <int FA, int FB>
+__device__ __forceinline__ void store_entry(const OutputView& out, uint64_t e, const uint32_t (&rt)[FA > 0 ? FA : 1],
+                                            const uint32_t (&ct)[FB > 0 ? FB : 1], double v) {
+    uint32_t* dst = out.idx + e * (FA + FB);
+    if constexpr (FA == 2 && FB == 2) {
+        __stcs(reinterpret_cast<uint4*>(dst), make_uint4(rt[0], rt[1], ct[0], ct[1]));
+    } else if constexpr (FA == 1 && FB == 1) {
+        __stcs(reinterpret_cast<uint2*>(dst), make_uint2(rt[0], ct[0]));
+    } else {
+        for (int k = 0; k < FA; ++k) dst[k] = rt[k];
+        for (int k = 0; k < FB; ++k) dst[FA + k] = ct[k];
+    }
+    __stcs(out.val + e, v);
+}
+
+// Emit n slots of the warp's table, listed in `list` (n <= kListCap), as output entries
+// base .. base + n - 1 (entry i holds list[i]), resetting those slots.  Every lane writes an
+// entry, so positions need no ballot; kEmitGroups 32-entry groups at a time, so their tuple loads
+// are in flight together.
+template <int FA, int FB>
+__device__ __forceinline__ void emit_list(const Operands& op, const OutputView& out, uint64_t base, uint32_t row,
+                                          uint32_t c0, bool dense, uint32_t n, const uint16_t* list, double* vals,
+                                          uint32_t* keys) {
     unsigned long long* vbits = reinterpret_cast<unsigned long long*>(vals);
     const uint32_t lane = lane_id();
     uint32_t rt[FA > 0 ? FA : 1];
     if (FA > 0)
         for (int m = 0; m < FA; ++m) rt[m] = op.row_tuple[(uint64_t)row * FA + m];
-    uint64_t o = base;
-    for (uint32_t i = 0; i < tsize; i += 32 * kEmitGroups) {
+    for (uint32_t i = 0; i < n; i += 32 * kEmitGroups) {
         bool occ[kEmitGroups];
         uint32_t col[kEmitGroups];
         double v[kEmitGroups];
-        uint32_t m[kEmitGroups];
 #pragma unroll
         for (int u = 0; u < kEmitGroups; ++u) {
-            const uint32_t sidx = i + u * 32 + lane;
-            occ[u] = false;
-            if (i + u * 32 < tsize) {
-                v[u] = vals[sidx];
-                occ[u] = __double_as_longlong(v[u]) != (long long)kNoValue;
-                col[u] = dense ? c0 + sidx : (occ[u] ? keys[sidx] : 0u);
-                if (occ[u]) {
-                    vbits[sidx] = kNoValue;
-                    if (!dense) keys[sidx] = kEmptyCol;
-                }
+            const uint32_t e = i + u * 32 + lane;
+            occ[u] = e < n;
+            if (occ[u]) {
+                const uint32_t slot = list[e];
+                v[u] = vals[slot];
+                col[u] = dense ? c0 + slot : keys[slot];
+                vbits[slot] = kNoValue;
+                if (!dense) keys[slot] = kEmptyCol;
             }
-            m[u] = __ballot_sync(kFullMask, occ[u]);
         }
         if (base == ~0ull) continue;  // rerun later: nothing written
         if (FA > 0) {
             uint32_t ct[kEmitGroups][FB > 0 ? FB : 1];
 #pragma unroll
             for (int u = 0; u < kEmitGroups; ++u)
-                if (occ[u])
-                    for (int k = 0; k < FB; ++k) ct[u][k] = op.col_tuple[(uint64_t)col[u] * FB + k];
+                if (occ[u]) load_col_tuple<FA, FB>(op, col[u], ct[u]);
 #pragma unroll
-            for (int u = 0; u < kEmitGroups; ++u) {
-                if (occ[u]) {
-                    const uint64_t e = o + __popc(m[u] & lanemask_lt());
-                    uint32_t* dst = out.idx + e * (FA + FB);
-                    if (FA == 2 && FB == 2) {
-                        __stcs(reinterpret_cast<uint4*>(dst), make_uint4(rt[0], rt[1], ct[u][0], ct[u][1]));
-                    } else if (FA == 1 && FB == 1) {
-                        __stcs(reinterpret_cast<uint2*>(dst), make_uint2(rt[0], ct[u][0]));
-                    } else {
-                        for (int k = 0; k < FA; ++k) dst[k] = rt[k];
-                        for (int k = 0; k < FB; ++k) dst[FA + k] = ct[u][k];
-                    }
-                    __stcs(out.val + e, v[u]);
-                }
-                o += __popc(m[u]);
-            }
+            for (int u = 0; u < kEmitGroups; ++u)
+                if (occ[u]) store_entry<FA, FB>(out, base + i + u * 32 + lane, rt, ct[u], v[u]);
         } else {
 #pragma unroll
-            for (int u = 0; u < kEmitGroups; ++u) {
-                if (occ[u]) write_entry(op, out, o + __popc(m[u] & lanemask_lt()), row, col[u], v[u]);
-                o += __popc(m[u]);
-            }
+            for (int u = 0; u < kEmitGroups; ++u)
+                if (occ[u]) write_entry(op, out, base + i + u * 32 + lane, row, col[u], v[u]);
         }
     }
+}
+
+// Refill the list with the next filled slots of the table, scanning from slot `scan` (a multiple
+// of 32) on while a whole 32-slot group still fits; returns how many were listed.  Emission of a
+// task that filled more slots than the list holds: the slots come out in slot order.
+__device__ __forceinline__ uint32_t list_refill(const double* vals, uint32_t tsize, uint16_t* list, uint32_t& scan) {
+    const unsigned long long* vbits = reinterpret_cast<const unsigned long long*>(vals);
+    uint32_t n = 0;
+    while (scan < tsize && n + 32 <= kListCap) {
+        const uint32_t sidx = scan + lane_id();
+        const bool occ = vbits[sidx] != kNoValue;
+        const uint32_t m = __ballot_sync(kFullMask, occ);
+        if (occ) list[n + __popc(m & lanemask_lt())] = (uint16_t)sidx;
+        n += __popc(m);
+        scan += 32;
+    }
+    __syncwarp();
+    return n;
+}
+
+// Appends the slots that lanes with `first` wrote first to the warp's list, in lane order; n counts
+// every such slot, also past the list's end.
+__device__ __forceinline__ void list_append(uint16_t* list, uint32_t& n, bool first, int slot) {
+    const uint32_t m = __ballot_sync(kFullMask, first);
+    if (m == 0) return;
+    if (first) {
+        const uint32_t p = n + __popc(m & lanemask_lt());
+        if (p < kListCap) list[p] = (uint16_t)slot;
+    }
+    n += __popc(m);
 }
 
 template <int FA, int FB>
@@ -481,9 +528,10 @@ __global__ void __launch_bounds__(kTaskWarps * 32, kTaskBlocksPerSm)
                      uint32_t* __restrict__ work_counter, uint32_t* __restrict__ overflow) {
     extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t warp = threadIdx.x >> 5, lane = lane_id();
-    double* vals = reinterpret_cast<double*>(smem + warp * kTaskBytes);
+    double* vals = reinterpret_cast<double*>(smem + warp * kWarpBytes);
     unsigned long long* vbits = reinterpret_cast<unsigned long long*>(vals);
     uint32_t* keys = reinterpret_cast<uint32_t*>(vals + kTaskSlots);
+    uint16_t* list = reinterpret_cast<uint16_t*>(smem + warp * kWarpBytes + kTaskBytes);
     for (uint32_t i = lane; i < kTaskDense; i += 32) vbits[i] = kNoValue;
     bool dense_layout = true;
     __syncwarp();
@@ -513,6 +561,7 @@ __global__ void __launch_bounds__(kTaskWarps * 32, kTaskBlocksPerSm)
         const uint32_t c0 = it.p0 << op.panel_log2;  // first column of the task
         const uint32_t ka = op.row_start[row], kb = op.row_start[row + 1];
         bool bad = false;  // table overflow or a column outside a dense task (never for exact sizes)
+        uint32_t filled = 0;  // slots written so far (warp-uniform); the first kListCap are listed
 
         for (uint32_t kw = ka; kw < kb; kw += 32) {
             const uint32_t k = kw + lane;
@@ -577,10 +626,12 @@ __global__ void __launch_bounds__(kTaskWarps * 32, kTaskBlocksPerSm)
                             if (!single) slot = __shfl_sync(kFullMask, slot, leader);
                         }
                         const uint32_t maxr = single ? 0u : __reduce_max_sync(kFullMask, valid ? rank : 0u);
+                        bool first = false;  // only a column's rank-0 product can find its slot empty
                         for (uint32_t r = 0; r <= maxr; ++r) {
-                            if (valid && rank == r && slot >= 0) accumulate(&vals[slot], prod);
+                            if (valid && rank == r && slot >= 0) first |= accumulate(&vals[slot], prod);
                             __syncwarp();
                         }
+                        list_append(list, filled, first, slot);
                     }
                 }
                 if (nl == 32) break;
@@ -601,16 +652,19 @@ __global__ void __launch_bounds__(kTaskWarps * 32, kTaskBlocksPerSm)
                     }
 #pragma unroll
                     for (int u = 0; u < kStreamUnroll; ++u) {
-                        if (cc[u] == kEmptyCol) continue;
-                        int slot;
-                        if (dense) {
-                            const uint32_t d = cc[u] - c0;
-                            slot = d < kTaskDense ? (int)d : -1;
-                        } else {
-                            slot = table_slot(keys, cc[u], tmask, tsize);
+                        int slot = -1;
+                        bool first = false;
+                        if (cc[u] != kEmptyCol) {
+                            if (dense) {
+                                const uint32_t d = cc[u] - c0;
+                                slot = d < kTaskDense ? (int)d : -1;
+                            } else {
+                                slot = table_slot(keys, cc[u], tmask, tsize);
+                            }
+                            if (slot < 0) bad = true;
+                            else first = accumulate(&vals[slot], __dmul_rn(ak, bv[u]));
                         }
-                        if (slot < 0) bad = true;
-                        else accumulate(&vals[slot], __dmul_rn(ak, bv[u]));
+                        list_append(list, filled, first, slot);
                     }
                 }
                 __syncwarp();  // the next A nonzero sees this one's values
@@ -621,9 +675,7 @@ __global__ void __launch_bounds__(kTaskWarps * 32, kTaskBlocksPerSm)
         // output position: exact, or claimed now that the count is known
         const bool any_bad = __any_sync(kFullMask, bad);
         uint64_t base = it.out_off;
-        uint32_t cnt = 0;
-        if (base == kClaimBit || out.item_count)
-            for (uint32_t i = 0; i < tsize; i += 32) cnt += __popc(__ballot_sync(kFullMask, vbits[i + lane] != kNoValue));
+        const uint32_t cnt = filled;  // every slot written is an output entry
         if (base == kClaimBit) {
             uint64_t b = ~0ull;
             if (lane == 0) {
@@ -639,7 +691,17 @@ __global__ void __launch_bounds__(kTaskWarps * 32, kTaskBlocksPerSm)
             base = ~0ull;
         }
         if (out.item_count && lane == 0) out.item_count[t] = base == ~0ull ? 0u : cnt;
-        emit_table<FA, FB>(op, out, base, row, c0, dense, tsize, vals, keys);
+        // the listed slots; a task that filled more slots than the list holds lists and emits them
+        // a part of the table at a time
+        const bool listed = filled <= kListCap;
+        uint32_t scan = listed ? tsize : 0u, n = listed ? filled : 0u;
+        for (;;) {
+            if (!listed) n = list_refill(vals, tsize, list, scan);
+            emit_list<FA, FB>(op, out, base, row, c0, dense, n, list, vals, keys);
+            if (scan >= tsize) break;
+            if (base != ~0ull) base += n;
+            __syncwarp();
+        }
         __syncwarp();
         t = __shfl_sync(kFullMask, tn, 0);
     }
@@ -648,7 +710,7 @@ __global__ void __launch_bounds__(kTaskWarps * 32, kTaskBlocksPerSm)
 void launch_warp_tasks(const Operands& op, const PartItem* tasks, uint32_t ntasks, const OutputView& out,
                        uint32_t* work_counter, uint32_t* overflow, int num_sms, cudaStream_t st) {
     if (ntasks == 0) return;
-    const size_t smem = kTaskWarps * kTaskBytes;
+    const size_t smem = kTaskWarps * kWarpBytes;
     PTC_CUDA(cudaMemsetAsync(work_counter, 0, sizeof(uint32_t), st));
     // the single-contraction layouts of the common free-mode counts get their own emission (the
     // general one also records rows and columns for the canonical order)
@@ -658,6 +720,8 @@ void launch_warp_tasks(const Operands& op, const PartItem* tasks, uint32_t ntask
     else if (plain && op.fa == 1 && op.fb == 1) kernel = warp_task_kernel<1, 1>;
     else if (plain && op.fa == 1 && op.fb == 2) kernel = warp_task_kernel<1, 2>;
     else if (plain && op.fa == 2 && op.fb == 1) kernel = warp_task_kernel<2, 1>;
+    // all of the SM's unified memory as shared memory: 8 blocks of 27 KiB
+    PTC_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     int per_sm = 1;
     PTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kTaskWarps * 32, smem));
     per_sm = per_sm < 1 ? 1 : per_sm;

@@ -30,7 +30,7 @@ uint32_t warp_task_max_bits();
 // column width of a dense warp task
 uint32_t warp_task_dense_columns();
 // rows whose A nonzeros number at most this go to warp tasks (they rescan the row once per task)
-constexpr uint32_t kWarpTaskMaxLen = 1024;
+constexpr uint32_t kWarpTaskMaxLen = 256;
 
 // other rows, numeric: one warp per task (a row's columns in fine panels [p0, p1))
 void launch_warp_tasks(const Operands& op, const PartItem* tasks, uint32_t ntasks, const OutputView& out,

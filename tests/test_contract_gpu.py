@@ -66,6 +66,19 @@ def test_against_oracle(engine, oracle_mod, case, kernel, path):
     assert_same_output(idx, vals, o["idx"], o["vals"], bit_exact=True)
 
 
+@pytest.mark.parametrize("path", ["two_phase", "learned"])
+def test_dense_tasks_fuller_than_the_slot_list(engine, oracle_mod, path):
+    """Rows of ~200 A nonzeros (warp tasks) over 2000 columns that all appear: dense tasks of 768
+    columns fill every slot, more than a warp's list of filled slots holds, so their emission
+    lists and writes the table a part at a time."""
+    t = gen.random_coo([60, 50, 2000], 400_000, [None] * 3, 39, "uniform01")
+    o = oracle_mod.contract(t, None, 2, [0, 1, 2])
+    idx, vals, st = engine.contract(t, None, 2, [0, 1, 2], large_rows="panels", path=path)
+    assert st["mult_adds"] == o["flops"]
+    assert st["out_nnz"] == o["nnz"] > 0.99 * 2000 * 2000
+    assert_same_output(idx, vals, o["idx"], o["vals"], bit_exact=True)
+
+
 def test_general_two_tensors(engine, oracle_mod):
     """A x B with different tensors and different mode positions (the reference's
     tc_fksCuckoo signature takes two tensors)."""
