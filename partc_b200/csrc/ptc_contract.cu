@@ -961,7 +961,8 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
     const uint32_t P = pl.P;
     stats.panel_width = pl.rowmap ? 0 : W;
     uint32_t* panel_off = nullptr;
-    if (P > 1 && table_bytes(W) <= kPanelTableBytes) {
+    // only the panel kernels read the table: none when no large row goes to them
+    if (P > 1 && n_big > pl.n_mapped && table_bytes(W) <= kPanelTableBytes) {
         panel_off = ar.alloc<uint32_t>(nfib * (uint64_t)(P + 1));
         launch_panel_offsets(op.b_col, op.fib_start, nfib, P, pl.log2w, panel_off, st);
     }
