@@ -38,6 +38,8 @@ sys.path.insert(0, ROOT)
 WORKLOAD = "zipf4d_3m"
 FALLBACK_HBM_GBS = 6650.0
 TUNE_SEED = 1001    # the autotuner's held-out tensor: the timed workload drawn with this seed
+L2_BYTES = 126 << 20     # B200 L2
+L2_FLUSH_BYTES = 512 << 20  # written before a step whose data would otherwise stay in L2
 CPU_WARMUP = 1      # reference runs before the timed ones (both CPU legs)
 CPU_STEPS = 3       # timed reference runs of the cpu_baseline leg (median)
 
@@ -127,14 +129,16 @@ def measured_hbm_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def traffic_from_profile():
-    """Per-launch DRAM bytes of the numeric pass from the committed ncu summary, if present."""
+def traffic_from_profile(workload: str):
+    """Per-launch DRAM bytes of the numeric pass from the committed ncu summary of this workload,
+    if there is one (profiles/numeric_traffic.json names the workload it was scaled to)."""
     p = os.path.join(ROOT, "profiles", "numeric_traffic.json")
     try:
         with open(p) as f:
-            return json.load(f)
+            d = json.load(f)
     except Exception:
         return None
+    return d if d.get("workload") == workload else None
 
 
 # ---------------------------------------------------------------------------------------------
@@ -636,16 +640,36 @@ def main():
     torch.cuda.synchronize()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
+    # a step that touches less than 4x the L2 (inputs + output) gets the L2 flushed before it,
+    # outside its timed span: each step is timed on its own and the spans are summed
+    touched = t.nnz * (4 * t.order + 8) + st0["out_nnz"] * (4 * 2 * (t.order - w.c) + 8)
+    flush = touched < 4 * L2_BYTES
+    l2_note = (f"L2 flushed before every step ({L2_FLUSH_BYTES >> 20} MiB written, untimed): a step touches "
+               f"{touched / 1e6:.0f} MB" if flush else
+               f"no flush needed: a step touches {touched / 1e9:.2f} GB (inputs + output, >> 126 MB L2)")
+    scrub = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=f"cuda:{local}") if flush else None
     stats = []
     with ClockSampler(local) as clk:
-        ev0.record(stream)
-        for _ in range(args.steps):
-            stats.append(step())
-        ev1.record(stream)
-        torch.cuda.synchronize()
+        if not flush:
+            ev0.record(stream)
+            for _ in range(args.steps):
+                stats.append(step())
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            span = ev0.elapsed_time(ev1)
+        else:
+            span = 0.0
+            for _ in range(args.steps):
+                with torch.cuda.stream(stream):
+                    scrub.fill_(1)
+                ev0.record(stream)
+                stats.append(step())
+                ev1.record(stream)
+                torch.cuda.synchronize()
+                span += ev0.elapsed_time(ev1)
     pdist.barrier()
     torch.cuda.synchronize()
-    ms = pdist.max_over_ranks(ev0.elapsed_time(ev1), device=f"cuda:{local}")
+    ms = pdist.max_over_ranks(span, device=f"cuda:{local}")
     M = stats[0]["mult_adds"]
     R = stats[0]["out_nnz"]
     value = pdist.job_throughput(M, args.steps, world, ms * 1e-3)
@@ -687,7 +711,7 @@ def main():
     t_num = statistics.mean(s["t_numeric_ms"] for s in stats) * 1e-3
     achieved = alg_bytes / t_num / 1e9
     peak, peak_kind = measured_hbm_peak()
-    traffic = traffic_from_profile()
+    traffic = traffic_from_profile(args.workload)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": peak_kind,
                 "kernel": numeric_kernels(stats[0]),
@@ -731,12 +755,12 @@ def main():
             "metric": "contraction mult-adds/s", "value": value, "unit": "mult-adds/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded generator partc_b200/gen.py: per-mode Zipf(1.1), U(0,1) values, seed 1)",
+            "data": f"synthetic (seeded generator partc_b200/gen.py, {args.workload}: {gen.describe(args.workload)})",
             "config": {"workload": w.name, "nnz": t.nnz, "dims": [int(x) for x in t.dims],
                        "contracted_modes": w.modes[:w.c], "path": args.path, "parallelism": f"replicas x{world}",
                        "knobs": knobs or "defaults",
                        "mult_adds_per_step": M, "out_nnz_per_step": R,
-                       "l2": "no flush needed: each step writes a 41 GB output (>> 126 MB L2)"},
+                       "l2": l2_note},
             "hbm_gbs_numeric": achieved,
             "phase_ms": {k: statistics.mean(s[k] for s in stats) for k in
                          ("t_build_ms", "t_symbolic_ms", "t_numeric_ms", "t_total_ms")},

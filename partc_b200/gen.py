@@ -183,6 +183,12 @@ WORKLOADS = {
 }
 
 
+def describe(name: str) -> str:
+    """One line on a named workload: the first sentence of its generator's docstring."""
+    doc = " ".join((WORKLOADS[name].__doc__ or name).split())
+    return doc.split(". ")[0].rstrip(".")
+
+
 def batch_member(seed: int) -> Workload:
     """One member of the uneven batch: 3-D or 4-D, dims 64-4096, nnz log-uniform in
     [1k, 200k], Zipf alpha in [0.8, 1.4] on every mode, U(-1,1) values, 1-2 contracted modes
