@@ -770,37 +770,42 @@ void launch_copy_rows(const Operands& op, const uint32_t* rows, uint32_t nrows, 
 }
 
 // ---------------------------------------------------------------------------------------------
-// numeric pass for the other rows: one block per part (a row's columns in fine panels [p0, p1)).
-// A dense part indexes its accumulator by column directly; a sparse part uses an open-addressing
-// table.  Both live in the same shared-memory region.
+// numeric pass for the rows of many A nonzeros: one block per part (a row's columns in fine
+// panels [p0, p1)).  The part's columns are dealt to the block's 16 warps (interleaved for a dense
+// part, by hash for a sparse one), and every warp keeps the columns it owns in a private table:
+// dense over 768 columns, or open addressing over 512 slots.
 //
-// The part's products are processed in segments of at most kSeg products, in stream order.  A
-// segment inside one A nonzero needs no ordering (its columns are distinct), and consecutive
-// segments of the same A nonzero need no barrier either.  A segment spanning several short A
-// nonzeros applies each column's products in stream order through claim rounds.
+// The part's products are taken in stream order, 512 per round (thread t: product pos + t).  A
+// round is split stably by owner warp into a shared buffer (a warp-level match_any gives each
+// product's rank among its warp's products of the same owner; per-(warp, owner) counts give the
+// buckets' offsets), then each warp applies its bucket -- its columns' products, still in stream
+// order -- 32 at a time with match_any ranks for equal columns, as a warp task does.  So every
+// column's products are applied by one warp in stream order, with three block barriers per round
+// and no claim rounds.
 // ---------------------------------------------------------------------------------------------
 
 constexpr int kPartThreads = 512;
-constexpr int kPartWarps = kPartThreads / 32;
-constexpr int kItems = 4;                              // products per thread per segment
-constexpr int kSeg = kPartThreads * kItems;            // 2048 products
-constexpr uint32_t kHashSlots = 8192;                  // sparse part: vals[8192] + keys[8192]
-constexpr uint32_t kDenseCols = 12288;                 // dense part: vals[12288] (same 96 KiB)
-constexpr uint32_t kClaimCells = 1024;
-constexpr uint32_t kNoClaim = 0xffffffffu;
-constexpr uint32_t kLongK = 256;                       // an A nonzero with this many products left
-                                                       // gets segments of its own
-constexpr size_t kRegionBytes = (size_t)kHashSlots * (sizeof(double) + sizeof(uint32_t));
-static_assert(kRegionBytes == kDenseCols * sizeof(double), "dense and sparse layouts share one region");
+constexpr int kPartWarps = kPartThreads / 32;            // 16 owners
+constexpr uint32_t kOwnDense = 768;                      // dense columns a warp owns
+constexpr uint32_t kOwnSlots = 512;                      // sparse slots a warp owns
+constexpr size_t kOwnBytes = kOwnDense * sizeof(double);  // a warp's table (6 KiB)
+static_assert(kOwnSlots * (sizeof(double) + sizeof(uint32_t)) <= kOwnBytes, "sparse layout fits a warp's region");
+constexpr uint32_t kDenseCols = kOwnDense * kPartWarps;   // 12288 columns in a dense part
+constexpr uint32_t kHashSlots = kOwnSlots * kPartWarps;   // 8192 slots in a sparse part
+constexpr uint32_t kPartWindow = 256;                     // A nonzeros read at a time
+constexpr size_t kRegionBytes = kOwnBytes * kPartWarps;   // 96 KiB of tables
+// behind the tables: a round's products by owner (column, value)
+constexpr size_t kPartSmemBytes = kRegionBytes + kPartThreads * (sizeof(uint32_t) + sizeof(double));
 
-uint32_t hash_part_capacity() { return kHashSlots * 3 / 4; }  // load factor <= 0.75
-uint32_t hash_part_min_bits() { return 9; }                    // 512 slots: 32 per warp
+// at most 5/8 of a sparse part's slots on average, so no warp's 512 slots fill up
+uint32_t hash_part_capacity() { return kHashSlots * 5 / 8; }
+uint32_t hash_part_min_bits() { return 13; }  // every sparse part has all 16 x 512 slots
 uint32_t dense_part_columns() { return kDenseCols; }
 
-// largest k in [lo, kPartThreads) with wscan[k] <= q (zero-length nonzeros share the next one's
+// largest k in [lo, kPartWindow) with wscan[k] <= q (zero-length nonzeros share the next one's
 // start, so this is the nonzero holding product q)
 __device__ __forceinline__ uint32_t find_nonzero(const uint32_t* wscan, uint32_t lo, uint32_t q) {
-    uint32_t hi = kPartThreads;
+    uint32_t hi = kPartWindow;
     while (hi - lo > 1) {
         const uint32_t mid = (lo + hi) >> 1;
         if (wscan[mid] <= q) lo = mid; else hi = mid;
@@ -808,24 +813,57 @@ __device__ __forceinline__ uint32_t find_nonzero(const uint32_t* wscan, uint32_t
     return lo;
 }
 
+// owner warp of a column of the part, and its slot hint: the local dense index, or the hash
+// bits above the owner's for the sparse table's first probe
+__device__ __forceinline__ uint32_t part_owner(uint32_t col, uint32_t lo, bool dense, uint32_t& hint) {
+    if (dense) {
+        const uint32_t d = col - lo;
+        hint = d >> 4;
+        return d & (kPartWarps - 1);
+    }
+    const uint32_t h = hash32(col);
+    hint = h >> 4;
+    return h & (kPartWarps - 1);
+}
+
+// Slot of column `col` in a warp's sparse table (linear probing from `hint`, inserted with
+// atomicCAS if absent), or -1 when the table is full.
+__device__ __forceinline__ int own_slot(uint32_t* keys, uint32_t col, uint32_t hint) {
+    uint32_t h = hint & (kOwnSlots - 1);
+    for (uint32_t probe = 0; probe < kOwnSlots; ++probe) {
+        const uint32_t cv = keys[h];
+        if (cv == col) return (int)h;
+        if (cv == kEmptyCol) {
+            const uint32_t old = atomicCAS(&keys[h], kEmptyCol, col);
+            if (old == kEmptyCol || old == col) return (int)h;
+        }
+        h = (h + 1) & (kOwnSlots - 1);
+    }
+    return -1;
+}
+
 __global__ void __launch_bounds__(kPartThreads, 2)
     hash_part_kernel(Operands op, const PartItem* __restrict__ parts, uint32_t nparts, OutputView out,
                      uint32_t* __restrict__ work_counter, uint32_t* __restrict__ overflow) {
     extern __shared__ __align__(16) unsigned char smem[];
-    double* vals = reinterpret_cast<double*>(smem);                                    // region
-    uint32_t* keys = reinterpret_cast<uint32_t*>(smem + kHashSlots * sizeof(double));  // sparse layout
-    uint32_t* claim = reinterpret_cast<uint32_t*>(smem + kRegionBytes);               // [kClaimCells]
-    __shared__ double wa[kPartThreads];
-    __shared__ uint32_t ws[kPartThreads], wl[kPartThreads], wscan[kPartThreads], nxt[kPartThreads];
+    const uint32_t t = threadIdx.x, lane = lane_id(), warp = t >> 5;
+    double* vals = reinterpret_cast<double*>(smem + warp * kOwnBytes);  // this warp's table
+    unsigned long long* vbits = reinterpret_cast<unsigned long long*>(vals);
+    uint32_t* keys = reinterpret_cast<uint32_t*>(vals + kOwnSlots);
+    double* bval = reinterpret_cast<double*>(smem + kRegionBytes);                     // a round's products,
+    uint32_t* bcol = reinterpret_cast<uint32_t*>(smem + kRegionBytes + kPartThreads * sizeof(double));  // by owner
+    __shared__ double wa[kPartWindow];
+    __shared__ uint32_t ws[kPartWindow], wscan[kPartWindow];
+    __shared__ uint32_t cnt[kPartWarps][kPartWarps];  // [warp][owner]: the round's products
+    __shared__ uint32_t off[kPartWarps][kPartWarps];  // [warp][owner]: their first buffer position
     __shared__ uint32_t tmp[kPartWarps + 1];
     __shared__ uint32_t wtot[kPartWarps];
     __shared__ uint32_t s_item;
     __shared__ uint64_t s_base;
-    const uint32_t t = threadIdx.x, lane = lane_id(), warp = t >> 5;
-    unsigned long long* vbits = reinterpret_cast<unsigned long long*>(vals);
 
-    for (uint32_t i = t; i < kClaimCells; i += kPartThreads) claim[i] = kNoClaim;
-    int layout = -1;  // 0 sparse, 1 dense (uniform)
+    for (uint32_t i = lane; i < kOwnDense; i += 32) vbits[i] = kNoValue;
+    bool dense_layout = true;
+    __syncwarp();
 
     for (;;) {
         __syncthreads();
@@ -835,29 +873,25 @@ __global__ void __launch_bounds__(kPartThreads, 2)
         if (item >= nparts) break;
         const PartItem it = parts[item];
         const bool dense = (it.mode & 1u) != 0;
-        const uint32_t tmask = dense ? 0u : (1u << (it.mode >> 1)) - 1u;
+        if (dense != dense_layout) {  // values are all empty after an emission; only keys differ
+            if (dense) {
+                for (uint32_t i = kOwnSlots + lane; i < kOwnDense; i += 32) vbits[i] = kNoValue;
+            } else {
+                for (uint32_t i = lane; i < kOwnSlots; i += 32) keys[i] = kEmptyCol;
+            }
+            dense_layout = dense;
+            __syncwarp();
+        }
         const uint32_t row = it.row;
         const uint32_t lo = it.p0 << op.panel_log2;  // first column of the part
-        if ((int)dense != layout) {
-            if (dense) {
-                for (uint32_t i = t; i < kDenseCols; i += kPartThreads) vbits[i] = kNoValue;
-            } else {
-                for (uint32_t i = t; i < kHashSlots; i += kPartThreads) {
-                    vbits[i] = kNoValue;
-                    keys[i] = kEmptyCol;
-                }
-            }
-            layout = dense;
-            __syncthreads();
-        }
         const uint32_t ka = op.row_start[row], kb = op.row_start[row + 1];
         bool bad = false;  // table overflow or a column outside a dense part (never for exact sizes)
 
-        for (uint32_t kw = ka; kw < kb; kw += kPartThreads) {
+        for (uint32_t kw = ka; kw < kb; kw += kPartWindow) {
             const uint32_t k = kw + t;
             uint32_t L = 0, s = 0;
             double a = 0.0;
-            if (k < kb) {
+            if (t < kPartWindow && k < kb) {
                 const int32_t f = op.a_fib[k];
                 if (f >= 0) {
                     uint32_t e;
@@ -868,144 +902,96 @@ __global__ void __launch_bounds__(kPartThreads, 2)
             }
             uint32_t total;
             const uint32_t excl = block_exclusive_scan<uint32_t, kPartThreads>(L, tmp, &total);
-            ws[t] = s;
-            wl[t] = L;
-            wscan[t] = excl;
-            wa[t] = a;
-            // nxt[k] = first nonzero >= k in this window with at least kLongK products
-            {
-                const uint32_t longmask = __ballot_sync(kFullMask, L >= kLongK);
-                if (lane == 0) tmp[warp] = longmask;  // free again: the scan has finished with it
+            if (t < kPartWindow) {
+                ws[t] = s;
+                wscan[t] = excl;
+                wa[t] = a;
+            }
+            __syncthreads();
+            uint32_t kk = 0;  // the window's A nonzero holding this thread's product
+            for (uint32_t pos = 0; pos < total; pos += kPartThreads) {
+                // thread t: product pos + t of the window's stream
+                const uint32_t q = pos + t;
+                uint32_t col = kEmptyCol, owner = kPartWarps, hint = 0;
+                double prod = 0.0;
+                if (q < total) {
+                    kk = find_nonzero(wscan, kk, q);
+                    const uint32_t j = ws[kk] + (q - wscan[kk]);
+                    col = __ldg(op.b_col + j);
+                    prod = __dmul_rn(wa[kk], __ldg(op.b_val + j));
+                    if (dense && col - lo >= kDenseCols) bad = true;
+                    else owner = part_owner(col, lo, dense, hint);
+                }
+                // stable split by owner: a product's rank among its warp's products of its owner,
+                // and per (warp, owner) counts
+                const uint32_t same = __match_any_sync(kFullMask, owner);
+                const uint32_t rank = __popc(same & lanemask_lt());
+                if (lane < kPartWarps) cnt[warp][lane] = 0;
+                __syncwarp();
+                if (owner < kPartWarps && rank == 0) cnt[warp][owner] = __popc(same);
                 __syncthreads();
-                const uint32_t m = longmask & ~lanemask_lt();
-                uint32_t n = kPartThreads;
-                if (m) {
-                    n = warp * 32 + __ffs(m) - 1;
-                } else {
-                    for (uint32_t w2 = warp + 1; w2 < kPartWarps; ++w2)
-                        if (tmp[w2]) { n = w2 * 32 + __ffs(tmp[w2]) - 1; break; }
-                }
-                nxt[t] = n;
-            }
-            __syncthreads();
-
-            uint32_t pos = 0;
-            while (pos < total) {
-                const uint32_t kcur = find_nonzero(wscan, 0, pos);  // uniform
-                const uint32_t kend = wscan[kcur] + wl[kcur];
-                uint32_t seg_end;
-                if (kend - pos >= kLongK) {
-                    seg_end = min(pos + (uint32_t)kSeg, kend);
-                } else {
-                    const uint32_t nl = (kcur + 1 < kPartThreads) ? nxt[kcur + 1] : kPartThreads;
-                    const uint32_t stop = nl < kPartThreads ? wscan[nl] : total;
-                    seg_end = min(min(pos + (uint32_t)kSeg, total), max(stop, kend));
-                }
-                const bool single = seg_end <= kend;
-                uint32_t col[kItems];
-                uint32_t slot[kItems];
-                double prod[kItems];
-                if (single) {
-                    // strided: consecutive threads read consecutive fiber entries
-                    const int64_t jb = (int64_t)ws[kcur] - (int64_t)wscan[kcur];
-                    const double ak = wa[kcur];
+                // warp o: owner o's bucket starts after the buckets of owners < o; inside it the
+                // warps' products follow in warp order
+                uint32_t bstart, bcount;
+                {
+                    const uint32_t* c = &cnt[0][0];
+                    uint32_t before = 0;
 #pragma unroll
-                    for (int i = 0; i < kItems; ++i) {
-                        const uint32_t q = pos + i * kPartThreads + t;
-                        col[i] = kEmptyCol;
-                        prod[i] = 0.0;
-                        if (q < seg_end) {
-                            const uint32_t j = (uint32_t)(jb + q);
-                            col[i] = op.b_col[j];
-                            prod[i] = __dmul_rn(ak, op.b_val[j]);
-                        }
+                    for (uint32_t m = 0; m < kPartWarps * kPartWarps / 32; ++m) {
+                        const uint32_t i = lane + 32 * m;
+                        if ((i & (kPartWarps - 1)) < warp) before += c[i];
                     }
-                } else {
-                    // blocked: thread t takes products [pos + t*kItems, ... + kItems)
-                    const uint32_t q0 = pos + t * kItems;
-                    uint32_t kk = q0 < seg_end ? find_nonzero(wscan, kcur, q0) : kcur;
-#pragma unroll
-                    for (int i = 0; i < kItems; ++i) {
-                        const uint32_t q = q0 + i;
-                        col[i] = kEmptyCol;
-                        prod[i] = 0.0;
-                        if (q < seg_end) {
-                            while (kk + 1 < kPartThreads && wscan[kk] + wl[kk] <= q) ++kk;
-                            const uint32_t j = ws[kk] + (q - wscan[kk]);
-                            col[i] = op.b_col[j];
-                            prod[i] = __dmul_rn(wa[kk], op.b_val[j]);
-                        }
-                    }
+                    before = warp_sum(before);
+                    const uint32_t mine = lane < kPartWarps ? cnt[lane][warp] : 0u;
+                    const uint32_t incl = warp_inclusive_scan(mine);
+                    if (lane < kPartWarps) off[lane][warp] = before + incl - mine;
+                    bstart = before;
+                    bcount = __shfl_sync(kFullMask, incl, 31);
                 }
-                // accumulator slot of every product
-#pragma unroll
-                for (int i = 0; i < kItems; ++i) {
-                    slot[i] = kEmptyCol;
-                    if (col[i] == kEmptyCol) continue;
-                    if (dense) {
-                        const uint32_t d = col[i] - lo;
-                        if (d < kDenseCols) slot[i] = d;
-                    } else {
-                        uint32_t h = hash32(col[i]) & tmask;
-                        for (uint32_t probe = 0; probe <= tmask; ++probe) {
-                            const uint32_t cur = keys[h];
-                            if (cur == col[i]) { slot[i] = h; break; }
-                            if (cur == kEmptyCol) {
-                                const uint32_t old = atomicCAS(&keys[h], kEmptyCol, col[i]);
-                                if (old == kEmptyCol || old == col[i]) { slot[i] = h; break; }
-                            }
-                            h = (h + 1) & tmask;
-                        }
-                    }
-                    if (slot[i] == kEmptyCol) { bad = true; col[i] = kEmptyCol; }
+                __syncthreads();
+                if (owner < kPartWarps) {
+                    const uint32_t d = off[warp][owner] + rank;
+                    bcol[d] = col;
+                    bval[d] = prod;
                 }
-                if (single) {
-#pragma unroll
-                    for (int i = 0; i < kItems; ++i)
-                        if (col[i] != kEmptyCol) accumulate(&vals[slot[i]], prod[i]);
-                    pos = seg_end;
-                    if (pos == kend) __syncthreads();  // the next segment starts another A nonzero
-                } else {
-                    // several A nonzeros: per column, apply in stream order (claim rounds)
-                    __syncthreads();
-                    bool pending[kItems];
-#pragma unroll
-                    for (int i = 0; i < kItems; ++i) pending[i] = col[i] != kEmptyCol;
-                    for (uint32_t round = 0; round < (uint32_t)kSeg + 1; ++round) {
-#pragma unroll
-                        for (int i = 0; i < kItems; ++i)
-                            if (pending[i]) atomicMin(&claim[slot[i] & (kClaimCells - 1)], t * kItems + i);
-                        __syncthreads();
-                        bool mine[kItems];
-#pragma unroll
-                        for (int i = 0; i < kItems; ++i)
-                            mine[i] = pending[i] && claim[slot[i] & (kClaimCells - 1)] == t * kItems + i;
-                        __syncthreads();
-                        bool left = false;
-#pragma unroll
-                        for (int i = 0; i < kItems; ++i) {
-                            if (mine[i]) {
-                                accumulate(&vals[slot[i]], prod[i]);
-                                claim[slot[i] & (kClaimCells - 1)] = kNoClaim;
-                                pending[i] = false;
-                            }
-                            left |= pending[i];
-                        }
-                        if (!__syncthreads_or(left)) break;
+                __syncthreads();
+                // this warp's bucket, in stream order, 32 products at a time; products meeting in
+                // one column apply by rank
+                for (uint32_t c0 = 0; c0 < bcount; c0 += 32) {
+                    const bool valid = c0 + lane < bcount;
+                    uint32_t cl = kEmptyCol;
+                    double p = 0.0;
+                    uint32_t h = 0;
+                    if (valid) {
+                        cl = bcol[bstart + c0 + lane];
+                        p = bval[bstart + c0 + lane];
+                        part_owner(cl, lo, dense, h);
                     }
-                    pos = seg_end;
+                    const uint32_t mm = __match_any_sync(kFullMask, cl);
+                    const uint32_t r = __popc(mm & lanemask_lt());
+                    int slot = -1;
+                    if (valid && r == 0) {
+                        slot = dense ? (int)h : own_slot(keys, cl, h);
+                        if (slot < 0) bad = true;
+                    }
+                    slot = __shfl_sync(kFullMask, slot, __ffs(mm) - 1);
+                    const uint32_t maxr = __reduce_max_sync(kFullMask, valid ? r : 0u);
+                    for (uint32_t rr = 0; rr <= maxr; ++rr) {
+                        if (valid && r == rr && slot >= 0) accumulate(&vals[slot], p);
+                        __syncwarp();
+                    }
                 }
             }
-            __syncthreads();
+            __syncthreads();  // the window's arrays are read again next window
         }
         const bool any_bad = __syncthreads_or(bad);
 
-        // emit: warp w owns slots [w * span, (w + 1) * span); dense parts come out in column order
-        const uint32_t span = (dense ? kDenseCols : tmask + 1) / kPartWarps;
-        uint32_t cnt = 0;
-        for (uint32_t i = 0; i < span; i += 32)
-            cnt += __popc(__ballot_sync(kFullMask, vbits[warp * span + i + lane] != kNoValue));
-        if (lane == 0) wtot[warp] = cnt;
+        // emit: warp w writes its table's entries after those of warps < w (a dense part's column
+        // of local slot l is lo + 16 l + w)
+        const uint32_t tsize = dense ? kOwnDense : kOwnSlots;
+        uint32_t n = 0;
+        for (uint32_t i = 0; i < tsize; i += 32) n += __popc(__ballot_sync(kFullMask, vbits[i + lane] != kNoValue));
+        if (lane == 0) wtot[warp] = n;
         __syncthreads();
         if (t == 0) {
             uint64_t base = it.out_off, total = 0;
@@ -1027,14 +1013,15 @@ __global__ void __launch_bounds__(kPartThreads, 2)
         const uint64_t base = s_base;
         uint64_t o = base;
         for (uint32_t w = 0; w < warp; ++w) o += wtot[w];
-        for (uint32_t i = 0; i < span; i += 32) {
-            const uint32_t sidx = warp * span + i + lane;
-            const bool occ = vbits[sidx] != kNoValue;
+        for (uint32_t i = 0; i < tsize; i += 32) {
+            const uint32_t sidx = i + lane;
+            const double v = vals[sidx];
+            const bool occ = __double_as_longlong(v) != (long long)kNoValue;
             const uint32_t m = __ballot_sync(kFullMask, occ);
             if (occ) {
                 if (base != ~0ull) {
-                    const uint32_t c = dense ? lo + sidx : keys[sidx];
-                    write_entry(op, out, o + __popc(m & lanemask_lt()), row, c, vals[sidx]);
+                    const uint32_t c = dense ? lo + (sidx << 4) + warp : keys[sidx];
+                    write_entry(op, out, o + __popc(m & lanemask_lt()), row, c, v);
                 }
                 vbits[sidx] = kNoValue;
                 if (!dense) keys[sidx] = kEmptyCol;
@@ -1047,9 +1034,10 @@ __global__ void __launch_bounds__(kPartThreads, 2)
 void launch_hash_parts(const Operands& op, const PartItem* parts, uint32_t nparts, const OutputView& out,
                        uint32_t* work_counter, uint32_t* overflow, int num_sms, cudaStream_t st) {
     if (nparts == 0) return;
-    const size_t smem = kRegionBytes + kClaimCells * sizeof(uint32_t);
+    const size_t smem = kPartSmemBytes;
     PTC_CUDA(cudaMemsetAsync(work_counter, 0, sizeof(uint32_t), st));
     PTC_CUDA(cudaFuncSetAttribute(hash_part_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    PTC_CUDA(cudaFuncSetAttribute(hash_part_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     int per_sm = 1;
     PTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hash_part_kernel, kPartThreads, smem));
     per_sm = per_sm < 1 ? 1 : per_sm;
