@@ -954,7 +954,7 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
         // above a sparse task's capacity becomes a dense task over that panel)
         while (2 * W <= warp_task_dense_columns() && panel_entries(W) * 4 > (2ull << 30)) W <<= 1;
     }
-    PTC_REQUIRE(pl.rowmap || W <= hash_part_capacity(), PTC_ERR_INVALID_ARGUMENT, "panel_width larger than a hash part");
+    PTC_REQUIRE(pl.rowmap || W <= dense_part_columns(), PTC_ERR_INVALID_ARGUMENT, "panel_width larger than a hash part");
     pl.W = W;
     pl.log2w = floor_log2(W);
     pl.P = (uint32_t)std::max<uint64_t>(1, (ncols + W - 1) / W);
@@ -985,8 +985,8 @@ Plan plan_rows(Front& F, const ptc_options& opt, const SizerHost* sizer, Collect
     br.dense_panels = dense_part_columns() >> pl.log2w;
     br.dense_min = W / kDenseMinFraction;
     br.min_bits = hash_part_min_bits();
-    br.max_bits = 13;
-    br.oversize_dense = 0;
+    br.max_bits = 12;
+    br.oversize_dense = 1;  // a panel above the capacity: a dense part over it
     br.load_num = 3;
     br.load_den = 4;
     if (pl.learned) {  // predicted sizes: every open-addressing table at its largest, for slack

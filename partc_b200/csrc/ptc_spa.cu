@@ -786,20 +786,23 @@ void launch_copy_rows(const Operands& op, const uint32_t* rows, uint32_t nrows, 
 
 constexpr int kPartThreads = 512;
 constexpr int kPartWarps = kPartThreads / 32;            // 16 owners
-constexpr uint32_t kOwnDense = 768;                      // dense columns a warp owns
-constexpr uint32_t kOwnSlots = 512;                      // sparse slots a warp owns
-constexpr size_t kOwnBytes = kOwnDense * sizeof(double);  // a warp's table (6 KiB)
+constexpr uint32_t kOwnDense = 384;                      // dense columns a warp owns
+constexpr uint32_t kOwnSlots = 256;                      // sparse slots a warp owns
+constexpr size_t kOwnBytes = kOwnDense * sizeof(double);  // a warp's table (3 KiB)
 static_assert(kOwnSlots * (sizeof(double) + sizeof(uint32_t)) <= kOwnBytes, "sparse layout fits a warp's region");
-constexpr uint32_t kDenseCols = kOwnDense * kPartWarps;   // 12288 columns in a dense part
-constexpr uint32_t kHashSlots = kOwnSlots * kPartWarps;   // 8192 slots in a sparse part
-constexpr uint32_t kPartWindow = 256;                     // A nonzeros read at a time
-constexpr size_t kRegionBytes = kOwnBytes * kPartWarps;   // 96 KiB of tables
-// behind the tables: a round's products by owner (column, value)
-constexpr size_t kPartSmemBytes = kRegionBytes + kPartThreads * (sizeof(uint32_t) + sizeof(double));
+constexpr uint32_t kDenseCols = kOwnDense * kPartWarps;   // 6144 columns in a dense part
+constexpr uint32_t kHashSlots = kOwnSlots * kPartWarps;   // 4096 slots in a sparse part
+constexpr uint32_t kPartWindow = 128;                     // A nonzeros read at a time
+constexpr int kRoundItems = 2;                            // products per thread in a round
+constexpr uint32_t kRound = kRoundItems * kPartThreads;   // products in a round
+constexpr size_t kRegionBytes = kOwnBytes * kPartWarps;   // 48 KiB of tables
+// behind the tables: a round's products by owner (value, column); 60 KiB in all, 3 blocks per SM
+constexpr size_t kPartSmemBytes = kRegionBytes + kRound * (sizeof(double) + sizeof(uint32_t));
 
-// at most 5/8 of a sparse part's slots on average, so no warp's 512 slots fill up
+// at most 5/8 of a sparse part's slots on average, so no warp's 256 slots fill up (a single
+// panel with more entries becomes a dense part over that panel)
 uint32_t hash_part_capacity() { return kHashSlots * 5 / 8; }
-uint32_t hash_part_min_bits() { return 13; }  // every sparse part has all 16 x 512 slots
+uint32_t hash_part_min_bits() { return 12; }  // every sparse part has all 16 x 256 slots
 uint32_t dense_part_columns() { return kDenseCols; }
 
 // largest k in [lo, kPartWindow) with wscan[k] <= q (zero-length nonzeros share the next one's
@@ -842,7 +845,7 @@ __device__ __forceinline__ int own_slot(uint32_t* keys, uint32_t col, uint32_t h
     return -1;
 }
 
-__global__ void __launch_bounds__(kPartThreads, 2)
+__global__ void __launch_bounds__(kPartThreads, 3)
     hash_part_kernel(Operands op, const PartItem* __restrict__ parts, uint32_t nparts, OutputView out,
                      uint32_t* __restrict__ work_counter, uint32_t* __restrict__ overflow) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -851,11 +854,11 @@ __global__ void __launch_bounds__(kPartThreads, 2)
     unsigned long long* vbits = reinterpret_cast<unsigned long long*>(vals);
     uint32_t* keys = reinterpret_cast<uint32_t*>(vals + kOwnSlots);
     double* bval = reinterpret_cast<double*>(smem + kRegionBytes);                     // a round's products,
-    uint32_t* bcol = reinterpret_cast<uint32_t*>(smem + kRegionBytes + kPartThreads * sizeof(double));  // by owner
+    uint32_t* bcol = reinterpret_cast<uint32_t*>(smem + kRegionBytes + kRound * sizeof(double));  // by owner
     __shared__ double wa[kPartWindow];
     __shared__ uint32_t ws[kPartWindow], wscan[kPartWindow];
-    __shared__ uint32_t cnt[kPartWarps][kPartWarps];  // [warp][owner]: the round's products
-    __shared__ uint32_t off[kPartWarps][kPartWarps];  // [warp][owner]: their first buffer position
+    __shared__ __align__(16) uint32_t cnt4[kRoundItems][kPartWarps][4];  // [item][warp]: bytes per owner
+    __shared__ uint16_t off[kRoundItems][kPartWarps][kPartWarps];        // [item][warp][owner]: buffer position
     __shared__ uint32_t tmp[kPartWarps + 1];
     __shared__ uint32_t wtot[kPartWarps];
     __shared__ uint32_t s_item;
@@ -908,52 +911,85 @@ __global__ void __launch_bounds__(kPartThreads, 2)
                 wa[t] = a;
             }
             __syncthreads();
-            uint32_t kk = 0;  // the window's A nonzero holding this thread's product
-            for (uint32_t pos = 0; pos < total; pos += kPartThreads) {
-                // thread t: product pos + t of the window's stream
-                const uint32_t q = pos + t;
-                uint32_t col = kEmptyCol, owner = kPartWarps, hint = 0;
-                double prod = 0.0;
-                if (q < total) {
-                    kk = find_nonzero(wscan, kk, q);
-                    const uint32_t j = ws[kk] + (q - wscan[kk]);
-                    col = __ldg(op.b_col + j);
-                    prod = __dmul_rn(wa[kk], __ldg(op.b_val + j));
-                    if (dense && col - lo >= kDenseCols) bad = true;
-                    else owner = part_owner(col, lo, dense, hint);
+            // Rounds of kRound products in stream order: product pos + i * 512 + t is thread t's
+            // item i.  A round's fiber entries are loaded during the round before, so their loads
+            // are in flight while that round's buckets are applied.
+            uint32_t kk = 0;  // the window's A nonzero holding this thread's latest product
+            uint32_t ncol[kRoundItems], nsrc[kRoundItems];
+            double nb[kRoundItems];
+            auto load_round = [&](uint32_t pos) {
+#pragma unroll
+                for (int i = 0; i < kRoundItems; ++i) {
+                    const uint32_t q = pos + i * kPartThreads + t;
+                    ncol[i] = kEmptyCol;
+                    nsrc[i] = 0;
+                    nb[i] = 0.0;
+                    if (q < total) {
+                        kk = find_nonzero(wscan, kk, q);
+                        const uint32_t j = ws[kk] + (q - wscan[kk]);
+                        ncol[i] = __ldg(op.b_col + j);
+                        nb[i] = __ldg(op.b_val + j);
+                        nsrc[i] = kk;
+                    }
                 }
-                // stable split by owner: a product's rank among its warp's products of its owner,
-                // and per (warp, owner) counts
-                const uint32_t same = __match_any_sync(kFullMask, owner);
-                const uint32_t rank = __popc(same & lanemask_lt());
-                if (lane < kPartWarps) cnt[warp][lane] = 0;
+            };
+            load_round(0);
+            for (uint32_t pos = 0; pos < total; pos += kRound) {
+                uint32_t col[kRoundItems], owner[kRoundItems], rank[kRoundItems];
+                double prod[kRoundItems];
+                if (lane < kRoundItems * 4) cnt4[lane >> 2][warp][lane & 3] = 0u;
                 __syncwarp();
-                if (owner < kPartWarps && rank == 0) cnt[warp][owner] = __popc(same);
+#pragma unroll
+                for (int i = 0; i < kRoundItems; ++i) {
+                    col[i] = ncol[i];
+                    owner[i] = kPartWarps;
+                    prod[i] = 0.0;
+                    if (col[i] != kEmptyCol) {
+                        uint32_t hint;
+                        prod[i] = __dmul_rn(wa[nsrc[i]], nb[i]);
+                        if (dense && col[i] - lo >= kDenseCols) bad = true;
+                        else owner[i] = part_owner(col[i], lo, dense, hint);
+                    }
+                    // stable split by owner: a product's rank among its warp's item-i products of
+                    // its owner, and per (item, warp, owner) counts (one byte each)
+                    const uint32_t same = __match_any_sync(kFullMask, owner[i]);
+                    rank[i] = __popc(same & lanemask_lt());
+                    if (owner[i] < kPartWarps && rank[i] == 0)
+                        reinterpret_cast<uint8_t*>(&cnt4[i][warp][0])[owner[i]] = (uint8_t)__popc(same);
+                }
                 __syncthreads();
                 // warp o: owner o's bucket starts after the buckets of owners < o; inside it the
-                // warps' products follow in warp order
+                // products follow in (item, warp) order: lane l of the scan is item l / 16, warp l % 16
                 uint32_t bstart, bcount;
                 {
-                    const uint32_t* c = &cnt[0][0];
+                    const uint32_t o = warp;
+                    const uint4 c = *reinterpret_cast<const uint4*>(&cnt4[lane >> 4][lane & 15][0]);
+                    const uint32_t w4[4] = {c.x, c.y, c.z, c.w};
                     uint32_t before = 0;
 #pragma unroll
-                    for (uint32_t m = 0; m < kPartWarps * kPartWarps / 32; ++m) {
-                        const uint32_t i = lane + 32 * m;
-                        if ((i & (kPartWarps - 1)) < warp) before += c[i];
+                    for (uint32_t k = 0; k < 4; ++k) {  // bytes of owners < o
+                        const uint32_t nbytes = o > 4 * k ? min(o - 4 * k, 4u) : 0u;
+                        const uint32_t mask = nbytes >= 4 ? 0xffffffffu : (1u << (8 * nbytes)) - 1u;
+                        before = __dp4a(w4[k] & mask, 0x01010101u, before);
                     }
                     before = warp_sum(before);
-                    const uint32_t mine = lane < kPartWarps ? cnt[lane][warp] : 0u;
+                    const uint32_t wo = o < 4 ? c.x : o < 8 ? c.y : o < 12 ? c.z : c.w;
+                    const uint32_t mine = (wo >> (8 * (o & 3))) & 0xffu;
                     const uint32_t incl = warp_inclusive_scan(mine);
-                    if (lane < kPartWarps) off[lane][warp] = before + incl - mine;
+                    off[lane >> 4][lane & 15][o] = (uint16_t)(before + incl - mine);
                     bstart = before;
                     bcount = __shfl_sync(kFullMask, incl, 31);
                 }
                 __syncthreads();
-                if (owner < kPartWarps) {
-                    const uint32_t d = off[warp][owner] + rank;
-                    bcol[d] = col;
-                    bval[d] = prod;
+#pragma unroll
+                for (int i = 0; i < kRoundItems; ++i) {
+                    if (owner[i] < kPartWarps) {
+                        const uint32_t d = off[i][warp][owner[i]] + rank[i];
+                        bcol[d] = col[i];
+                        bval[d] = prod[i];
+                    }
                 }
+                if (pos + kRound < total) load_round(pos + kRound);
                 __syncthreads();
                 // this warp's bucket, in stream order, 32 products at a time; products meeting in
                 // one column apply by rank
