@@ -364,8 +364,8 @@ uint32_t warp_task_min_bits() { return 6; }                   // 64 slots: two p
 uint32_t warp_task_max_bits() { return 9; }
 
 // A sub-range of at least this many products is streamed on its own (see warp_task_kernel)
-constexpr uint32_t kStreamMin = 16;
-constexpr int kStreamUnroll = 4;
+constexpr uint32_t kStreamMin = 32;
+constexpr int kStreamUnroll = 2;
 
 // Slot of column `col` in an open-addressing table of tmask + 1 = tsize slots (linear probing,
 // inserted with atomicCAS if absent), or -1 when the table is full.
