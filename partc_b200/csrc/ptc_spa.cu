@@ -773,12 +773,12 @@ void launch_copy_rows(const Operands& op, const uint32_t* rows, uint32_t nrows, 
 // numeric pass for the rows of many A nonzeros: one block per part (a row's columns in fine
 // panels [p0, p1)).  The part's columns are dealt to the block's 16 warps (interleaved for a dense
 // part, by hash for a sparse one), and every warp keeps the columns it owns in a private table:
-// dense over 768 columns, or open addressing over 512 slots.
+// dense over 384 columns, or open addressing over 256 slots.
 //
-// The part's products are taken in stream order, 512 per round (thread t: product pos + t).  A
-// round is split stably by owner warp into a shared buffer (a warp-level match_any gives each
-// product's rank among its warp's products of the same owner; per-(warp, owner) counts give the
-// buckets' offsets), then each warp applies its bucket -- its columns' products, still in stream
+// The part's products are taken in stream order, 1024 per round (thread t: products pos + t and
+// pos + 512 + t).  A round is split stably by owner warp into a shared buffer (a warp-level
+// match_any gives each product's rank among its warp's products of the same owner; per-(item,
+// warp, owner) counts give the buckets' offsets), then each warp applies its bucket -- its columns' products, still in stream
 // order -- 32 at a time with match_any ranks for equal columns, as a warp task does.  So every
 // column's products are applied by one warp in stream order, with three block barriers per round
 // and no claim rounds.
