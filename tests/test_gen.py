@@ -46,3 +46,9 @@ def test_batch_member_shapes():
         assert 1 <= w.c <= 2
         assert (64 <= w.tensor.dims).all() and (w.tensor.dims <= 4096).all()
         assert 1 <= w.tensor.nnz <= 200_000
+
+
+def test_every_named_workload_has_a_one_line_description():
+    for name in gen.WORKLOADS:
+        d = gen.describe(name)
+        assert d and "\n" not in d and not d.endswith(".")
